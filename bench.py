@@ -1,0 +1,459 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 assembly engine.
+
+Default workload (N=1): vector P2 linear elasticity on UnitCubeMesh(48,48,48)
+(663,552 tetrahedra, 2,738,019 dofs, 231,797,385 CSR non-zeros), interior
+vertices jittered by a seeded uniform +-0.15h, E = 1, nu = 0.3, body force
+(0,0,-1).  One step = SystemAssembler-style assembly of A and b in one pass
+(FP64), inputs resident in HBM.  Also measured on the same data: the
+FP32-contraction path (max relative error vs the FP64 result) and the
+matrix-free action y = A x.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl reference]
+
+Prints ONE JSON line (rank 0).  Multi-GPU (torchrun): every rank assembles
+its own independently seeded mesh (weak scaling, no collective on the data
+path); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Assembly Mcells/s, FP32/batched vs plain FP64 GPU at <=1e-6 rel err; %HBM peak"
+
+WORKLOADS = {
+    # name: (kind, n, degree, description)
+    "elasticity_p2_48": ("elasticity", 48, 2, "vector P2 elasticity, UnitCubeMesh(48) jittered 0.15h, A+b"),
+    "poisson_p1_32": ("poisson", 32, 1, "P1 Poisson kappa P1 + load f P1, UnitCubeMesh(32), A+b"),
+    "poisson_p2_96": ("poisson", 96, 2, "P2 Poisson kappa P1 + load f P1, UnitCubeMesh(96), A+b"),
+}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = f"/tmp/db2_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 8:
+                    continue
+                try:
+                    sm.append(float(f[0]))
+                    smax = float(f[1])
+                except ValueError:
+                    continue
+                for nm, val in zip(names, f[4:8]):
+                    if val.lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def setup_workload(name, seed, device):
+    import torch
+    import dolfin_b200 as d2
+    from dolfin_b200 import synthetic
+    kind, n, deg, _ = WORKLOADS[name]
+    t0 = time.perf_counter()
+    mesh = d2.UnitCubeMesh(n, n, n)
+    x0 = mesh.coordinates()
+    if kind == "elasticity":
+        x = synthetic.jitter_interior(x0, n, 0.15, seed)
+        mesh.set_coordinates(x)
+        V = d2.VectorFunctionSpace(mesh, "Lagrange", deg)
+        u, v = d2.TrialFunction(V), d2.TestFunction(V)
+        E, nu = 1.0, 0.3
+        mu = d2.Constant(E / (2 * (1 + nu)))
+        lmbda = d2.Constant(E * nu / ((1 + nu) * (1 - 2 * nu)))
+        eps = lambda w: d2.sym(d2.grad(w))
+        sigma = lambda w: 2 * mu * eps(w) + lmbda * d2.tr(eps(w)) * d2.Identity(3)
+        a = d2.inner(sigma(u), eps(v)) * d2.dx
+        L = d2.inner(d2.Constant((0.0, 0.0, -1.0)), v) * d2.dx
+        fields = {}
+    else:
+        x = x0
+        V = d2.FunctionSpace(mesh, "Lagrange", deg)
+        W = d2.FunctionSpace(mesh, "Lagrange", 1)
+        kv = synthetic.uniform_field(mesh.num_vertices(), 0.5, 2.0, seed)
+        fv = synthetic.uniform_field(mesh.num_vertices(), -1.0, 1.0, seed + 1)
+        kappa, f = d2.Function(W, kv), d2.Function(W, fv)
+        u, v = d2.TrialFunction(V), d2.TestFunction(V)
+        a = kappa * d2.inner(d2.grad(u), d2.grad(v)) * d2.dx
+        L = f * v * d2.dx
+        fields = {"kappa": kv, "f": fv}
+    S = d2.SystemAssembler(a, L)
+    A, b = d2.Matrix(), d2.Vector(n=V.dim())
+    S.assemble(A, b)  # builds the pattern and the plan, first assembly
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    return dict(mesh=mesh, V=V, a=a, L=L, S=S, A=A, b=b, x=x, fields=fields, kind=kind, n=n,
+                deg=deg, setup_s=setup_s)
+
+
+def algorithmic_bytes(w):
+    """8 nnz (value write) + 8 N (b write) + 4 (d+1) C (cell->vertex map)
+    + 8 gdim Nv (coordinates) + 8 Nv per P1 field read."""
+    mesh, V, A = w["mesh"], w["V"], w["A"]
+    C, Nv = mesh.num_cells(), mesh.num_vertices()
+    B = 8 * A.nnz() + 8 * V.dim() + 4 * 4 * C + 8 * 3 * Nv + 8 * Nv * len(w["fields"])
+    return B
+
+
+def time_steps(fn, steps, flush=None):
+    """Per-step CUDA-event device time (ms) of fn() on the current stream."""
+    import torch
+    evs = []
+    for _ in range(steps):
+        if flush is not None:
+            flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        fn()
+        e.record()
+        evs.append((s, e))
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in evs]
+
+
+def cpu_baseline_sample(w, target_s=10.0, threads=1):
+    """The oracle (CPU restatement of DOLFIN's serial assemble_cells loop with
+    coeffRef-style CSR insertion) on the first cells of the same mesh."""
+    from oracle import oracle as orc
+    mesh = w["mesh"]
+    om = orc.Mesh(3, np.ascontiguousarray(w["x"]), mesh.cells())
+    deg = w["deg"]
+    vs = 3 if w["kind"] == "elasticity" else 1
+    od, N = orc.dofmap(om, deg, vs)
+    S = 2048 if w["kind"] == "elasticity" else (8192 if deg == 2 else 65536)
+    sub = orc.Mesh(3, om.coords, om.cells[:S])
+    dsub = np.ascontiguousarray(od[:S])
+    rp, cols = orc.sparsity(N, N, dsub, dsub)
+    if w["kind"] == "elasticity":
+        fa = orc.form(orc.ELASTICITY, 3, deg, 3, mu=1 / 2.6, lmbda=0.3 / (1.3 * 0.4))
+        fl = orc.form(orc.LOAD, 3, deg, 3, coeff=orc.COEFF_CONST, c=(0, 0, -1))
+        wa = wl = None
+    else:
+        fa = orc.form(orc.DIFFUSION, 3, deg, 1, coeff=orc.COEFF_P1)
+        fl = orc.form(orc.LOAD, 3, deg, 1, coeff=orc.COEFF_P1)
+        wa, wl = w["fields"]["kappa"], w["fields"]["f"]
+    reps, t = 0, 0.0
+    while t < target_s:
+        t0 = time.perf_counter()
+        orc.assemble_matrix(fa, sub, dsub, dsub, rp, cols, w=wa)
+        orc.assemble_vector(fl, sub, dsub, N, w=wl)
+        t += time.perf_counter() - t0
+        reps += 1
+    return {"value": S * reps / t / 1e6, "unit": "Mcells/s", "cores": threads, "kind": "port",
+            "sample": f"first {S} cells of the workload mesh, A+b, {reps} passes, {t:.1f} s"}
+
+
+# ---------------------------------------------------------------------------
+# Reference arm: the reference's algorithm on the host cores.  DOLFIN itself
+# cannot be built here (it needs FFC/UFL, Boost, Eigen, MPI); its serial
+# assembly path is restated in oracle/ (C++) and run on every host core, one
+# process per core over disjoint cell ranges of the same workload.
+# ---------------------------------------------------------------------------
+_REF = {}
+
+
+def _ref_init(workload, rank, ncells):
+    from oracle import oracle as orc
+    from dolfin_b200 import synthetic
+    kind, n, deg, _ = WORKLOADS[workload]
+    om = orc.unit_cube_mesh(n, n, n)
+    vs = 3 if kind == "elasticity" else 1
+    if kind == "elasticity":
+        om.coords = synthetic.jitter_interior(om.coords, n, 0.15, 1000)
+        fa = orc.form(orc.ELASTICITY, 3, deg, 3, mu=1 / 2.6, lmbda=0.3 / (1.3 * 0.4))
+        fl = orc.form(orc.LOAD, 3, deg, 3, coeff=orc.COEFF_CONST, c=(0, 0, -1))
+        wa = wl = None
+    else:
+        fa = orc.form(orc.DIFFUSION, 3, deg, 1, coeff=orc.COEFF_P1)
+        fl = orc.form(orc.LOAD, 3, deg, 1, coeff=orc.COEFF_P1)
+        wa = synthetic.uniform_field(om.nv, 0.5, 2.0, 1000)
+        wl = synthetic.uniform_field(om.nv, -1.0, 1.0, 1001)
+    od, N = orc.dofmap(om, deg, vs)
+    lo = (rank * ncells) % om.nc
+    sub = orc.Mesh(3, om.coords, np.ascontiguousarray(om.cells[lo:lo + ncells]))
+    dsub = np.ascontiguousarray(od[lo:lo + ncells])
+    rp, cols = orc.sparsity(N, N, dsub, dsub)
+    _REF.update(orc=orc, sub=sub, dsub=dsub, rp=rp, cols=cols, fa=fa, fl=fl, wa=wa, wl=wl, N=N)
+
+
+def _ref_work(_):
+    r = _REF
+    t0 = time.perf_counter()
+    r["orc"].assemble_matrix(r["fa"], r["sub"], r["dsub"], r["dsub"], r["rp"], r["cols"], w=r["wa"])
+    r["orc"].assemble_vector(r["fl"], r["sub"], r["dsub"], r["N"], w=r["wl"])
+    return time.perf_counter() - t0
+
+
+def _ref_worker_main(workload, rank, ncells, steps, warmup, q_in, q_out):
+    _ref_init(workload, rank, ncells)
+    q_out.put("ready")
+    while True:
+        msg = q_in.get()
+        if msg is None:
+            return
+        q_out.put(_ref_work(None))
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    kind, n, deg, desc = WORKLOADS[args.workload]
+    ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    per = {"elasticity": 512, "poisson": 32768 if deg == 1 else 4096}[kind]
+    procs, qin, qout = [], [], []
+    for r in range(ncores):
+        qi, qo = ctx.Queue(), ctx.Queue()
+        p = ctx.Process(target=_ref_worker_main, args=(args.workload, r, per, args.steps, args.warmup, qi, qo))
+        p.start()
+        procs.append(p)
+        qin.append(qi)
+        qout.append(qo)
+    for qo in qout:
+        assert qo.get(timeout=900) == "ready"
+
+    def step():
+        t0 = time.perf_counter()
+        for qi in qin:
+            qi.put(1)
+        for qo in qout:
+            qo.get(timeout=900)
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        step()
+    times = [step() for _ in range(args.steps)]
+    for qi in qin:
+        qi.put(None)
+    for p in procs:
+        p.join(timeout=60)
+    t = float(np.mean(times))
+    value = ncores * per / t / 1e6
+    line = {
+        "metric": METRIC, "impl": "reference", "value": round(value, 4), "unit": "Mcells/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; same mesh and fields)",
+        "config": {"workload": args.workload, "description": desc},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mcells/s", "cores": ncores, "kind": "port",
+                         "sample": f"{per} cells per core x {ncores} cores per step (disjoint ranges), "
+                                   "oracle restatement of DOLFIN's serial assemble_cells + EigenMatrix::add"},
+        "e2e": {"value": round(value, 4), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="elasticity_p2_48", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import dolfin_b200 as d2
+    from dolfin_b200 import _capi
+
+    w = setup_workload(args.workload, seed=1000 + rank, device=local)
+    S, A, b = w["S"], w["A"], w["b"]
+    cells = w["mesh"].num_cells()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        S.assemble(A, b)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    l0 = _capi.kernel_launches()
+    with ClockSampler(local) as clk:
+        t_wall0 = time.perf_counter()
+        ms = time_steps(step, args.steps, flush)
+        t_wall = time.perf_counter() - t_wall0
+    launches = _capi.kernel_launches() - l0
+    if dist:
+        dist.barrier()
+    ms_step = float(np.mean(ms))
+    if dist:
+        t = torch.tensor([ms_step], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = cells * world / (ms_step * 1e-3) / 1e6
+
+    # roofline of the dominant kernel (the assembly kernel is the only launch per step)
+    peak, peak_kind = load_peaks()
+    B = algorithmic_bytes(w)
+    achieved = B / (ms_step * 1e-3) / 1e9
+
+    # FP32 contraction path on the same data
+    vals64 = A.values_tensor().clone()
+    b64 = b.tensor().clone()
+    S32 = d2.SystemAssembler(w["a"], w["L"], precision="fp32")
+    A32, b32 = d2.Matrix(w["V"].pattern()), d2.Vector(n=w["V"].dim())
+    S32.assemble(A32, b32)
+    for _ in range(args.warmup):
+        S32.assemble(A32, b32)
+    ms32 = float(np.mean(time_steps(lambda: S32.assemble(A32, b32), args.steps, flush)))
+    err32 = float((A32.values_tensor() - vals64).abs().max().item() / vals64.abs().max().item())
+
+    # matrix-free action on the same form
+    x = torch.randn(w["V"].dim(), dtype=torch.float64, device="cuda",
+                    generator=torch.Generator("cuda").manual_seed(7))
+    y = d2.Vector(n=w["V"].dim())
+    for _ in range(args.warmup):
+        d2.assemble_action(w["a"], d2.Vector(x), y)
+    ms_mf = float(np.mean(time_steps(lambda: d2.assemble_action(w["a"], d2.Vector(x), y), args.steps, flush)))
+
+    # end to end through the public API with host buffers: per step, H2D of the
+    # step's input (vertex coordinates for elasticity, kappa and f otherwise)
+    # and D2H of the result (CSR values and b)
+    nnz = A.nnz()
+    h_vals = torch.empty(nnz, dtype=torch.float64, pin_memory=True)
+    h_b = torch.empty(w["V"].dim(), dtype=torch.float64, pin_memory=True)
+    if w["kind"] == "elasticity":
+        h_in = [torch.from_numpy(np.ascontiguousarray(w["x"])).pin_memory()]
+    else:
+        h_in = [torch.from_numpy(w["fields"]["kappa"]).pin_memory(),
+                torch.from_numpy(w["fields"]["f"]).pin_memory()]
+    mesh = w["mesh"]
+
+    def e2e_step():
+        if w["kind"] == "elasticity":
+            mesh.set_coordinates(h_in[0].numpy())  # host -> device coordinate upload
+        else:
+            fs = [c for c in w["a"].coefficients()[0]] + [c for c in w["L"].coefficients()[0]]
+            for fobj, hsrc in zip(fs, h_in):
+                fobj.tensor().copy_(hsrc, non_blocking=True)
+        S.assemble(A, b)
+        h_vals.copy_(A.values_tensor(), non_blocking=True)
+        h_b.copy_(b.tensor(), non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    e2e_step()
+    t0 = time.perf_counter()
+    n_e2e = max(3, min(args.steps, 10))
+    for _ in range(n_e2e):
+        e2e_step()
+    e2e_ms = (time.perf_counter() - t0) / n_e2e * 1e3
+    h2d = sum(t.numel() * 8 for t in h_in)
+    d2h = (nnz + w["V"].dim()) * 8
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(w)
+
+    if rank == 0:
+        _, n, deg, desc = WORKLOADS[args.workload]
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mcells/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded jittered unit-cube mesh; no external dataset)",
+            "config": {"workload": args.workload, "description": desc, "cells": cells,
+                       "dofs": w["V"].dim(), "nnz": nnz, "precision": "fp64",
+                       "l2": "flushed between steps (256 MiB write)", "setup_s": round(w["setup_s"], 2),
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "peak_source": peak_kind, "algorithmic_bytes": B},
+            "fp32_contract": {"value": round(cells / (ms32 * 1e-3) / 1e6, 3), "unit": "Mcells/s",
+                              "ms_per_step": round(ms32, 4), "speedup_vs_fp64": round(ms_step / ms32, 3),
+                              "max_rel_err_vs_fp64": err32},
+            "matrix_free": {"ms_per_action": round(ms_mf, 4),
+                            "mcells_s": round(cells / (ms_mf * 1e-3) / 1e6, 3)},
+            "e2e": {"value": round(cells / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mcells/s",
+                    "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "wall_s_timed_region": round(t_wall, 3),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,275 @@
+// action.cu -- matrix-free action y = A x and the adjoint (VJP) with respect
+// to a P1 coefficient, on the same row-gather plan as assembly.
+#include <cuda_runtime.h>
+
+#include "launch.cuh"
+
+namespace db2 {
+namespace dev {
+
+// Local edge index of the unordered local vertex pair (p, q), p != q.
+template <int D>
+__device__ __forceinline__ int edge_of(int p, int q) {
+  const int lo = p < q ? p : q, hi = p < q ? q : p;
+  if constexpr (D == 3) {
+    // (2,3)->0 (1,3)->1 (1,2)->2 (0,3)->3 (0,2)->4 (0,1)->5
+    if (lo == 0) return hi == 1 ? 5 : (hi == 2 ? 4 : 3);
+    if (lo == 1) return hi == 2 ? 2 : 1;
+    return 0;
+  } else {
+    // (1,2)->0 (0,2)->1 (0,1)->2
+    if (lo == 0) return hi == 1 ? 2 : 1;
+    return 0;
+  }
+}
+
+// Global nodes of the relabelled cell in its local order (vertices = vertex
+// ids; P2 edge nodes through the cell's node list).
+template <int D, int P>
+__device__ __forceinline__ void relabelled_nodes(const AsmParams& p, uint32_t cell, uint32_t code,
+                                                 const uint32_t (&pv)[D + 1],
+                                                 uint32_t (&nodes)[El<D, P>::K]) {
+  using E = El<D, P>;
+  for (int a = 0; a <= D; ++a) nodes[a] = pv[a];
+  if constexpr (P == 2) {
+    const uint32_t* cn = p.cell_nodes + size_t(cell) * E::K;
+    for (int e2 = 0; e2 < E::NE; ++e2) {
+      const int A = edge_end(D, e2, 0), B = edge_end(D, e2, 1);
+      const int pa = int((code >> (2 * A)) & 3u), pb = int((code >> (2 * B)) & 3u);
+      nodes[E::NV + e2] = __ldg(cn + E::NV + edge_of<D>(pa, pb));
+    }
+  }
+}
+
+// y[(c,i)] = sum over cells K around node i of sum_{e,j} A^K_{(c,i),(e,j)} x[(e,j)]
+// (one thread per dof row, register accumulation in cell order).
+template <int D, int P, int FORM, bool KP1, typename CT>
+__global__ void __launch_bounds__(256) k_apply(const AsmParams p, const double* __restrict__ xin,
+                                               double* __restrict__ y) {
+  using E = El<D, P>;
+  constexpr int BS = FORM == FORM_ELAS ? D : 1;
+  const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= p.nnodes * BS) return;
+  const int c = int(r / p.nnodes);
+  const int64_t node = r - int64_t(c) * p.nnodes;
+  double acc = 0.0;
+  for (uint32_t ii = __ldg(p.inc_ptr + node); ii < __ldg(p.inc_ptr + node + 1); ++ii) {
+    const uint32_t word = __ldg(p.inc + ii);
+    const uint32_t cell = word & 0x0fffffffu;
+    const int li = int(word >> 28);
+    uint32_t pv[D + 1], code;
+    load_cell<D>(p, cell, li, pv, code);
+    double x[D + 1][D];
+    load_coords<D>(p, pv, x);
+    double kap[D + 1];
+    if constexpr (KP1)
+      for (int a = 0; a <= D; ++a) kap[a] = __ldg(p.kappa + pv[a]);
+    Geometry<D> G;
+    geometry(x, G);
+    uint32_t nodes[E::K];
+    relabelled_nodes<D, P>(p, cell, code, pv, nodes);
+#pragma unroll 1
+    for (int e = 0; e < BS; ++e) {
+      CT out[E::K];
+      element_row<D, P, FORM, KP1, CT>(p, G, li <= D, c, e, kap, out);
+      const double* xe = xin + int64_t(e) * p.nnodes;
+#pragma unroll
+      for (int j = 0; j < E::K; ++j) acc = fma(double(out[j]), __ldg(xe + nodes[j]), acc);
+    }
+  }
+  y[r] = acc;
+}
+
+// Adjoint, step 1 (one thread per cell): t[cell][m] = sum_{i,j in cell}
+// gA_ij dA^K_ij/dkappa_m + sum_i gb_i db^K_i/dkappa_m for the P1 kappa
+// basis functions m of the cell.
+template <int D, int P, bool LOADK, typename CT>
+__global__ void __launch_bounds__(256) k_vjp_cells(const AsmParams p, int64_t ncells,
+                                                   const double* __restrict__ gA,
+                                                   const double* __restrict__ gb,
+                                                   double* __restrict__ t) {
+  using E = El<D, P>;
+  using R = Rows<D, P, CT>;
+  constexpr int NB = D + 1;
+  const int64_t cell = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (cell >= ncells) return;
+  double acc[NB];
+  for (int a = 0; a < NB; ++a) acc[a] = 0.0;
+  const uint32_t* cn = p.cell_nodes + size_t(cell) * E::K;
+  for (int li = 0; li < E::K; ++li) {
+    const uint32_t ii = __ldg(p.cell_inc + size_t(cell) * E::K + li);
+    const uint32_t node = __ldg(cn + li);
+    const double* grow = gA + __ldg(p.node_rowptr + node);
+    uint32_t pv[D + 1], code;
+    load_cell<D>(p, uint32_t(cell), li, pv, code);
+    double x[D + 1][D];
+    load_coords<D>(p, pv, x);
+    Geometry<D> G;
+    geometry(x, G);
+    const bool vertex = li <= D;
+    // gA at the row's slots, in the relabelled local order
+    const uint32_t* pw = reinterpret_cast<const uint32_t*>(p.pos + size_t(ii) * E::KP);
+    double g[E::K];
+    for (int q = 0; q < E::KP / 4; ++q) {
+      const uint32_t w = __ldg(pw + q);
+      for (int s = 0; s < 4; ++s)
+        if (4 * q + s < E::K) g[4 * q + s] = __ldg(grow + ((w >> (8 * s)) & 0xffu));
+    }
+    CT W0[1][NB];
+    CT W1[2][NB];
+    for (int b = 0; b < NB; ++b) W0[0][b] = CT(G.vol * gdot<D>(G, 0, b) * p.kscale);
+    if constexpr (P == 2)
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < NB; ++b) W1[a][b] = CT(G.vol * gdot<D>(G, a, b) * p.kscale);
+    double fv[NB];
+    if constexpr (LOADK)
+      for (int a = 0; a < NB; ++a) fv[a] = __ldg(p.f + pv[a]);
+    CT lk[NB];
+    if constexpr (LOADK) {
+      CT fc[NB];
+      for (int a = 0; a < NB; ++a) fc[a] = CT(fv[a]);
+      if constexpr (P == 2) {
+        if (vertex) R::v_kfp1(fc, lk);
+        else R::e_kfp1(fc, lk);
+      } else {
+        R::v_kfp1(fc, lk);
+      }
+    }
+    const double gbi = LOADK ? __ldg(gb + node) : 0.0;
+    for (int m = 0; m < NB; ++m) {
+      CT unit[NB];
+      for (int a = 0; a < NB; ++a) unit[a] = CT(a == m ? 1 : 0);
+      CT d[E::K];
+      if (P == 1 || vertex) R::v_kp1(W0, unit, d);
+      else if constexpr (P == 2) R::e_kp1(W1, unit, d);
+      double s = 0.0;
+      for (int j = 0; j < E::K; ++j) s = fma(g[j], double(d[j]), s);
+      if constexpr (LOADK) s = fma(gbi, G.vol * double(lk[m]) * p.fc[0], s);
+      // relabelled vertex m is original local vertex perm[m]
+      const int orig = int((code >> (2 * m)) & 3u);
+      for (int a = 0; a < NB; ++a)
+        if (a == orig) acc[a] += s;
+    }
+  }
+  for (int a = 0; a < NB; ++a) t[cell * NB + a] = acc[a];
+}
+
+// Adjoint, step 2 (one thread per vertex): dkappa[v] = sum over cells around
+// v, in cell order, of t[cell][local index of v].
+template <int D>
+__global__ void __launch_bounds__(256) k_vjp_vertices(const AsmParams p, int64_t nv,
+                                                      const double* __restrict__ t,
+                                                      double* __restrict__ dk) {
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  double s = 0.0;
+  for (uint32_t ii = __ldg(p.inc_ptr + v); ii < __ldg(p.inc_ptr + v + 1); ++ii) {
+    const uint32_t word = __ldg(p.inc + ii);
+    s += __ldg(t + size_t(word & 0x0fffffffu) * (D + 1) + (word >> 28));
+  }
+  dk[v] = s;
+}
+
+template <int D, int P, int FORM, bool KP1, typename CT>
+void run_apply(const AsmParams& p, int bs, const double* x, double* y, cudaStream_t s) {
+  const int64_t n = p.nnodes * bs;
+  k_apply<D, P, FORM, KP1, CT><<<unsigned((n + 255) / 256), 256, 0, s>>>(p, x, y);
+  count_launch();
+  check_cuda("apply launch");
+}
+
+}  // namespace dev
+
+dev::AsmParams make_params(const Pattern& P);
+
+void launch_apply(const Pattern& P, const FormArgs& a, int precision, const double* x, double* y,
+                  void* stream) {
+  dev::AsmParams p = make_params(P);
+  const int D = P.V->mesh->tdim, deg = P.V->degree;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool fp32 = precision == DB2_FP32_CONTRACT;
+  if (precision != DB2_FP64 && !fp32) fail(DB2_ERR_ARGUMENT, "unknown precision %d", precision);
+  bool kp1 = false;
+  if (a.f.kind == DB2_FORM_DIFFUSION) {
+    if (P.bs != 1) fail(DB2_ERR_UNSUPPORTED, "diffusion form on a vector space");
+    p.kscale = a.f.coeff == DB2_COEFF_CONSTANT || a.f.coeff == DB2_COEFF_P1_SCALED ? a.f.constant[0] : 1.0;
+    kp1 = a.f.coeff == DB2_COEFF_P1 || a.f.coeff == DB2_COEFF_P1_SCALED;
+    if (kp1 && !a.w) fail(DB2_ERR_ARGUMENT, "P1 coefficient field missing");
+    p.kappa = a.w;
+#define DB2_AP(D_, P_)                                                                  \
+  if (D == D_ && deg == P_) {                                                           \
+    if (kp1) {                                                                          \
+      if (fp32) dev::run_apply<D_, P_, dev::FORM_DIFF, true, float>(p, 1, x, y, s);     \
+      else dev::run_apply<D_, P_, dev::FORM_DIFF, true, double>(p, 1, x, y, s);         \
+    } else {                                                                            \
+      if (fp32) dev::run_apply<D_, P_, dev::FORM_DIFF, false, float>(p, 1, x, y, s);    \
+      else dev::run_apply<D_, P_, dev::FORM_DIFF, false, double>(p, 1, x, y, s);        \
+    }                                                                                   \
+    return;                                                                             \
+  }
+    DB2_AP(3, 1) DB2_AP(3, 2) DB2_AP(2, 1) DB2_AP(2, 2)
+#undef DB2_AP
+  } else if (a.f.kind == DB2_FORM_ELASTICITY) {
+    if (D != 3 || P.bs != 3) fail(DB2_ERR_UNSUPPORTED, "elasticity needs a 3D vector space");
+    p.mu = a.f.mu;
+    p.lmbda = a.f.lmbda;
+    if (deg == 1) {
+      if (fp32) dev::run_apply<3, 1, dev::FORM_ELAS, false, float>(p, 3, x, y, s);
+      else dev::run_apply<3, 1, dev::FORM_ELAS, false, double>(p, 3, x, y, s);
+    } else {
+      if (fp32) dev::run_apply<3, 2, dev::FORM_ELAS, false, float>(p, 3, x, y, s);
+      else dev::run_apply<3, 2, dev::FORM_ELAS, false, double>(p, 3, x, y, s);
+    }
+    return;
+  }
+  fail(DB2_ERR_UNSUPPORTED, "matrix-free action not provided for this form/element");
+}
+
+size_t vjp_scratch_doubles(const Pattern& P) {
+  return size_t(P.V->mesh->nc) * (P.V->mesh->tdim + 1);
+}
+
+void launch_vjp(const Pattern& P, const FormArgs& a, const FormArgs& L, int precision,
+                const double* gA, const double* gb, double* dkappa, double* scratch,
+                void* stream) {
+  if (a.f.kind != DB2_FORM_DIFFUSION || P.bs != 1)
+    fail(DB2_ERR_UNSUPPORTED, "the adjoint is provided for kappa*grad(u).grad(v)*dx on scalar spaces");
+  if (!(a.f.coeff == DB2_COEFF_P1 || a.f.coeff == DB2_COEFF_P1_SCALED))
+    fail(DB2_ERR_ARGUMENT, "the adjoint is with respect to a P1 kappa");
+  const bool fp32 = precision == DB2_FP32_CONTRACT;
+  if (precision != DB2_FP64 && !fp32) fail(DB2_ERR_ARGUMENT, "unknown precision %d", precision);
+  dev::AsmParams p = make_params(P);
+  p.kscale = a.f.coeff == DB2_COEFF_P1_SCALED ? a.f.constant[0] : 1.0;
+  p.kappa = a.w;
+  // L = kappa * f * v * dx contributes when its coefficient is P1_SCALED
+  // (the kappa-weighted load); any other load does not depend on kappa.
+  const bool loadk = gb && L.f.kind == DB2_FORM_LOAD && L.f.coeff == DB2_COEFF_P1_SCALED;
+  if (loadk) {
+    if (!L.w) fail(DB2_ERR_ARGUMENT, "kappa-weighted load needs its P1 field f");
+    p.f = L.w;
+    p.fc[0] = 1.0;
+  }
+  const int D = P.V->mesh->tdim, deg = P.V->degree;
+  const int64_t nc = P.V->mesh->nc, nv = P.V->mesh->nv;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const unsigned bc = unsigned((nc + 255) / 256), bv = unsigned((nv + 255) / 256);
+#define DB2_VJP(D_, P_)                                                                        \
+  if (D == D_ && deg == P_) {                                                                  \
+    if (loadk) {                                                                               \
+      if (fp32) dev::k_vjp_cells<D_, P_, true, float><<<bc, 256, 0, s>>>(p, nc, gA, gb, scratch); \
+      else dev::k_vjp_cells<D_, P_, true, double><<<bc, 256, 0, s>>>(p, nc, gA, gb, scratch);  \
+    } else {                                                                                   \
+      if (fp32) dev::k_vjp_cells<D_, P_, false, float><<<bc, 256, 0, s>>>(p, nc, gA, gb, scratch); \
+      else dev::k_vjp_cells<D_, P_, false, double><<<bc, 256, 0, s>>>(p, nc, gA, gb, scratch); \
+    }                                                                                          \
+    dev::k_vjp_vertices<D_><<<bv, 256, 0, s>>>(p, nv, scratch, dkappa);                         \
+    count_launch(2);                                                                           \
+    check_cuda("vjp launch");                                                                  \
+    return;                                                                                    \
+  }
+  DB2_VJP(3, 1) DB2_VJP(3, 2) DB2_VJP(2, 1) DB2_VJP(2, 2)
+#undef DB2_VJP
+  fail(DB2_ERR_UNSUPPORTED, "adjoint not provided for this element");
+}
+
+}  // namespace db2

@@ -1,0 +1,11 @@
+// Instantiations: vector elasticity (+ constant body force) on tetrahedra, P1 and P2.
+#include "launch.cuh"
+namespace db2 {
+namespace dev {
+bool dispatch_tet_elas(int P, const AsmParams& p, const LaunchCfg& cfg, bool kp1, int loadm, bool fp32) {
+  if (P == 1) return dispatch<3, 1, FORM_ELAS>(p, cfg, kp1, loadm, fp32);
+  if (P == 2) return dispatch<3, 2, FORM_ELAS>(p, cfg, kp1, loadm, fp32);
+  return false;
+}
+}  // namespace dev
+}  // namespace db2

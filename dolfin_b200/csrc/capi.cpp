@@ -1,0 +1,327 @@
+// capi.cpp -- the extern "C" boundary: status codes instead of exceptions,
+// opaque handles, thread-local error messages.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "internal.h"
+
+struct db2_mesh_t {
+  std::shared_ptr<db2::Mesh> m;
+};
+struct db2_space_t {
+  std::shared_ptr<db2::Space> V;
+};
+struct db2_pattern_t {
+  std::shared_ptr<db2::Pattern> P;
+  db2::DeviceBuffer scratch;  // adjoint work array (grown on demand)
+};
+
+namespace db2 {
+int64_t launches();
+}
+
+namespace {
+thread_local std::string g_err;
+
+template <typename F>
+int guard(F&& f) {
+  try {
+    f();
+    return DB2_OK;
+  } catch (const db2::Error& e) {
+    g_err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_err = "host allocation failed";
+    return DB2_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return DB2_ERR_ARGUMENT;
+  } catch (...) {
+    g_err = "unknown error";
+    return DB2_ERR_ARGUMENT;
+  }
+}
+
+void need(const void* p, const char* what) {
+  if (!p) db2::fail(DB2_ERR_ARGUMENT, "%s is NULL", what);
+}
+
+db2::FormArgs form_args(const db2_form* f, const double* w) {
+  db2::FormArgs a;
+  a.f = *f;
+  a.w = w;
+  return a;
+}
+}  // namespace
+
+extern "C" {
+
+const char* db2_last_error(void) { return g_err.c_str(); }
+const char* db2_version(void) { return "dolfin_b200 0.1 (sm_100a)"; }
+int64_t db2_kernel_launches(void) { return db2::launches(); }
+
+int db2_mesh_create(int tdim, int64_t nv, const double* coords, int64_t nc, const uint32_t* cells,
+                    db2_mesh* out) {
+  return guard([&] {
+    need(out, "out");
+    auto h = new db2_mesh_t{db2::make_mesh(tdim, nv, coords, nc, cells)};
+    *out = h;
+  });
+}
+
+int db2_mesh_unit_cube(int nx, int ny, int nz, db2_mesh* out) {
+  return guard([&] {
+    need(out, "out");
+    *out = new db2_mesh_t{db2::make_unit_cube(nx, ny, nz)};
+  });
+}
+
+int db2_mesh_unit_square(int nx, int ny, int diagonal, db2_mesh* out) {
+  return guard([&] {
+    need(out, "out");
+    *out = new db2_mesh_t{db2::make_unit_square(nx, ny, diagonal)};
+  });
+}
+
+int db2_mesh_info(db2_mesh m, int* tdim, int64_t* nv, int64_t* nc) {
+  return guard([&] {
+    need(m, "mesh");
+    if (tdim) *tdim = m->m->tdim;
+    if (nv) *nv = m->m->nv;
+    if (nc) *nc = m->m->nc;
+  });
+}
+
+int db2_mesh_copy(db2_mesh m, double* coords, uint32_t* cells) {
+  return guard([&] {
+    need(m, "mesh");
+    if (coords) std::memcpy(coords, m->m->x.data(), m->m->x.size() * sizeof(double));
+    if (cells) std::memcpy(cells, m->m->cells.data(), m->m->cells.size() * sizeof(uint32_t));
+  });
+}
+
+int db2_mesh_set_coordinates(db2_mesh m, const double* coords) {
+  return guard([&] {
+    need(m, "mesh");
+    need(coords, "coords");
+    std::memcpy(m->m->x.data(), coords, m->m->x.size() * sizeof(double));
+    if (m->m->on_device) m->m->upload_coordinates();
+  });
+}
+
+int db2_mesh_num_edges(db2_mesh m, int64_t* ne) {
+  return guard([&] {
+    need(m, "mesh");
+    need(ne, "ne");
+    m->m->compute_edges();
+    *ne = m->m->ne;
+  });
+}
+
+int db2_mesh_destroy(db2_mesh m) {
+  delete m;
+  return DB2_OK;
+}
+
+int db2_space_create(db2_mesh m, int degree, int value_size, db2_space* out) {
+  return guard([&] {
+    need(m, "mesh");
+    need(out, "out");
+    *out = new db2_space_t{db2::make_space(m->m, degree, value_size)};
+  });
+}
+
+int db2_space_info(db2_space V, int* ndofs_per_cell, int64_t* dim) {
+  return guard([&] {
+    need(V, "space");
+    if (ndofs_per_cell) *ndofs_per_cell = V->V->k * V->V->vsize;
+    if (dim) *dim = V->V->dim();
+  });
+}
+
+// DofMap::cell_dofs: component-major local order, dof = c*nnodes + node.
+int db2_space_cell_dofs(db2_space V, int32_t* out) {
+  return guard([&] {
+    need(V, "space");
+    need(out, "out");
+    const auto& S = *V->V;
+    const int k = S.k, n = k * S.vsize;
+    for (int64_t c = 0; c < S.mesh->nc; ++c)
+      for (int comp = 0; comp < S.vsize; ++comp)
+        for (int i = 0; i < k; ++i)
+          out[c * n + comp * k + i] = int32_t(comp * S.nnodes + S.cell_nodes[c * k + i]);
+  });
+}
+
+int db2_space_destroy(db2_space V) {
+  delete V;
+  return DB2_OK;
+}
+
+int db2_pattern_create(db2_space V, int keep_diagonal, db2_pattern* out) {
+  return guard([&] {
+    need(V, "space");
+    need(out, "out");
+    auto h = new db2_pattern_t;
+    try {
+      h->P = db2::make_pattern(V->V, keep_diagonal != 0);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int db2_pattern_info(db2_pattern P, int64_t* nrows, int64_t* nnz) {
+  return guard([&] {
+    need(P, "pattern");
+    if (nrows) *nrows = P->P->nrows;
+    if (nnz) *nnz = P->P->nnz;
+  });
+}
+
+int db2_pattern_csr_device(db2_pattern P, const int32_t** rowptr, const int32_t** cols) {
+  return guard([&] {
+    need(P, "pattern");
+    P->P->ensure_device();
+    if (rowptr) *rowptr = P->P->d_rowptr.as<int32_t>();
+    if (cols) *cols = P->P->d_cols.as<int32_t>();
+  });
+}
+
+int db2_pattern_csr_host(db2_pattern P, int32_t* rowptr, int32_t* cols) {
+  return guard([&] {
+    need(P, "pattern");
+    P->P->csr_host(rowptr, cols);
+  });
+}
+
+int db2_pattern_plan_info(db2_pattern P, int64_t* nnodes, int64_t* nincidences, int* kp,
+                          int64_t* ntiles) {
+  return guard([&] {
+    need(P, "pattern");
+    if (nnodes) *nnodes = P->P->V->nnodes;
+    if (nincidences) *nincidences = int64_t(P->P->inc.size());
+    if (kp) *kp = P->P->kp;
+    if (ntiles) *ntiles = int64_t(P->P->tiles.size());
+  });
+}
+
+int db2_pattern_plan_copy(db2_pattern P, int32_t* node_rowptr, int32_t* node_cols,
+                          uint32_t* inc_ptr, uint32_t* inc, uint8_t* pos, int32_t* tiles) {
+  return guard([&] {
+    need(P, "pattern");
+    const auto& Q = *P->P;
+    if (node_rowptr) std::memcpy(node_rowptr, Q.node_rowptr.data(), Q.node_rowptr.size() * 4);
+    if (node_cols) std::memcpy(node_cols, Q.node_cols.data(), Q.node_cols.size() * 4);
+    if (inc_ptr) std::memcpy(inc_ptr, Q.inc_ptr.data(), Q.inc_ptr.size() * 4);
+    if (inc) std::memcpy(inc, Q.inc.data(), Q.inc.size() * 4);
+    if (pos) std::memcpy(pos, Q.pos.data(), Q.pos.size());
+    if (tiles) std::memcpy(tiles, Q.tiles.data(), Q.tiles.size() * sizeof(db2::Tile));
+  });
+}
+
+int db2_pattern_retile(db2_pattern P, int tile_threads, int seg_cap_bytes) {
+  return guard([&] {
+    need(P, "pattern");
+    db2::retile(*P->P, tile_threads, seg_cap_bytes);
+  });
+}
+
+int db2_pattern_destroy(db2_pattern P) {
+  delete P;
+  return DB2_OK;
+}
+
+int db2_assemble_matrix(db2_pattern P, const db2_form* a, const double* w, int precision,
+                        double* vals, int add_values, void* stream) {
+  return guard([&] {
+    need(P, "pattern");
+    need(a, "form");
+    need(vals, "vals");
+    const db2::FormArgs fa = form_args(a, w);
+    db2::launch_assemble(*P->P, &fa, nullptr, precision, vals, nullptr, add_values != 0, nullptr,
+                         nullptr, stream);
+  });
+}
+
+int db2_assemble_vector(db2_pattern P, const db2_form* L, const double* w, double* b,
+                        int add_values, void* stream) {
+  return guard([&] {
+    need(P, "pattern");
+    need(L, "form");
+    need(b, "b");
+    const db2::FormArgs fl = form_args(L, w);
+    db2::launch_assemble(*P->P, nullptr, &fl, DB2_FP64, nullptr, b, add_values != 0, nullptr,
+                         nullptr, stream);
+  });
+}
+
+int db2_assemble_system(db2_pattern P, const db2_form* a, const double* wa, const db2_form* L,
+                        const double* wL, int precision, double* vals, double* b, void* stream) {
+  return guard([&] {
+    need(P, "pattern");
+    need(a, "bilinear form");
+    need(L, "linear form");
+    need(vals, "vals");
+    need(b, "b");
+    const db2::FormArgs fa = form_args(a, wa), fl = form_args(L, wL);
+    db2::launch_assemble(*P->P, &fa, &fl, precision, vals, b, false, nullptr, nullptr, stream);
+  });
+}
+
+int db2_assemble_system_bc(db2_pattern P, const db2_form* a, const double* wa, const db2_form* L,
+                           const double* wL, const uint8_t* bc_flags, const double* bc_vals,
+                           int precision, double* vals, double* b, void* stream) {
+  return guard([&] {
+    need(P, "pattern");
+    need(a, "bilinear form");
+    need(L, "linear form");
+    need(bc_flags, "bc_flags");
+    need(bc_vals, "bc_vals");
+    const db2::FormArgs fa = form_args(a, wa), fl = form_args(L, wL);
+    db2::launch_assemble(*P->P, &fa, &fl, precision, vals, b, false, bc_flags, bc_vals, stream);
+  });
+}
+
+int db2_apply(db2_pattern P, const db2_form* a, const double* w, int precision, const double* x,
+              double* y, void* stream) {
+  return guard([&] {
+    need(P, "pattern");
+    need(a, "form");
+    need(x, "x");
+    need(y, "y");
+    db2::launch_apply(*P->P, form_args(a, w), precision, x, y, stream);
+  });
+}
+
+int db2_vjp_kappa(db2_pattern P, const db2_form* a, const double* kappa, const db2_form* L,
+                  const double* f, const double* gA, const double* gb, int precision,
+                  double* dkappa, void* stream) {
+  return guard([&] {
+    need(P, "pattern");
+    need(a, "form");
+    need(kappa, "kappa");
+    need(gA, "gA");
+    need(dkappa, "dkappa");
+    const size_t need_d = db2::vjp_scratch_doubles(*P->P);
+    if (P->scratch.bytes < need_d * sizeof(double)) P->scratch.alloc(need_d * sizeof(double));
+    db2::FormArgs fl;
+    if (L) fl = form_args(L, f);
+    else {
+      std::memset(&fl.f, 0, sizeof(fl.f));
+      fl.f.kind = DB2_FORM_LOAD;
+      fl.f.coeff = DB2_COEFF_NONE;
+    }
+    db2::launch_vjp(*P->P, form_args(a, kappa), fl, precision, gA, L ? gb : nullptr, dkappa,
+                    P->scratch.as<double>(), stream);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,136 @@
+// internal.h -- host-side data structures of the engine (not part of the ABI).
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/dolfin_b200.h"
+
+namespace db2 {
+
+// Thrown inside the library, converted to a status code at the C boundary.
+struct Error {
+  int code;
+  std::string msg;
+};
+[[noreturn]] void fail(int code, const char* fmt, ...);
+
+// Device buffer with RAII release (cudaFree); defined in device.cu.
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer();
+  void alloc(size_t nbytes);
+  void upload(const void* host, size_t nbytes);  // alloc + synchronous copy
+  template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// ---- mesh ----------------------------------------------------------------
+struct Mesh {
+  int tdim = 0;
+  int64_t nv = 0, nc = 0;
+  std::vector<double> x;         // nv * tdim
+  std::vector<uint32_t> cells;   // nc * (tdim+1), sorted per cell
+  // edges (computed on demand): numbered in sorted (v0<v1) key order
+  bool have_edges = false;
+  int64_t ne = 0;
+  std::vector<uint32_t> cell_edges;  // nc * nedges(tdim), UFC local edge order
+  // device copies: coordinates padded to 4 (3D) or 2 (2D) doubles per vertex
+  DeviceBuffer d_x, d_cells;
+  bool on_device = false;
+  void ensure_device();      // first GPU use: upload coordinates and cells
+  void upload_coordinates();
+  void compute_edges();
+};
+
+int nverts(int tdim);
+int nedges(int tdim);
+
+// ---- function space ---------------------------------------------------------
+struct Space {
+  std::shared_ptr<Mesh> mesh;
+  int degree = 1, vsize = 1;
+  int k = 0;              // nodes (scalar dofs) per cell
+  int64_t nnodes = 0;     // scalar global dimension
+  std::vector<uint32_t> cell_nodes;  // nc * k
+  DeviceBuffer d_cell_nodes;
+  bool on_device = false;
+  void ensure_device();
+  int64_t dim() const { return nnodes * vsize; }
+};
+
+// ---- sparsity pattern + row-gather plan -------------------------------------
+// Node-level graph (the scalar pattern); the dof-level CSR of a vector space
+// is its component expansion: row (c,i) = [c'*nnodes + j for c' in 0..bs-1
+// for j in nodecols(i)], rowptr(c,i) = c*bs*nnz_node + bs*node_rowptr[i].
+struct Tile {
+  int32_t comp;   // test component c of the tile's rows
+  int32_t n0, n1; // node range [n0, n1)
+  int32_t pad;
+};
+
+struct Pattern {
+  std::shared_ptr<Space> V;
+  bool keep_diagonal = false;
+  int bs = 1;
+  int64_t nnz_node = 0, nnz = 0, nrows = 0;
+  std::vector<int32_t> node_rowptr;  // nnodes + 1
+  std::vector<int32_t> node_cols;    // nnz_node
+  // row-gather plan: node -> incident (cell, local node) in ascending cell order
+  int kp = 0;                        // pos bytes per incidence (k rounded up to 4)
+  std::vector<uint32_t> inc_ptr;     // nnodes + 1
+  std::vector<uint32_t> inc;         // cell | local_node << 28
+  std::vector<uint8_t> pos;          // inc.size() * kp: column slot (within the node row)
+                                     // of each node of the relabelled cell
+  std::vector<uint32_t> cell_inc;    // nc * k: incidence index of (cell, local node)
+  std::vector<Tile> tiles;
+  int tile_threads = 128;
+  int seg_cap = 0;                   // doubles of shared memory per tile
+  DeviceBuffer d_node_rowptr, d_inc_ptr, d_inc, d_pos, d_cell_inc, d_tiles, d_rowptr, d_cols;
+  bool on_device = false;
+  void ensure_device();      // first GPU use: upload the plan, expand the CSR
+  // dof-level CSR on the host (component expansion of the node graph)
+  void csr_host(int32_t* rowptr, int32_t* cols) const;
+};
+
+// Relabelling of a cell so that local node `li` becomes canonical: for a
+// vertex node, that vertex first and the others ascending; for an edge node
+// (p,q), p and q first.  perm[a] = original local vertex at new position a.
+void canonical_perm(int tdim, int li, int perm[4]);
+// map[j] = original local node of the relabelled cell's local node j.
+void canonical_node_map(int tdim, int degree, int li, int* map);
+
+std::shared_ptr<Mesh> make_unit_cube(int nx, int ny, int nz);
+std::shared_ptr<Mesh> make_unit_square(int nx, int ny, int diagonal);
+std::shared_ptr<Mesh> make_mesh(int tdim, int64_t nv, const double* x, int64_t nc,
+                                const uint32_t* cells);
+std::shared_ptr<Space> make_space(std::shared_ptr<Mesh> m, int degree, int vsize);
+std::shared_ptr<Pattern> make_pattern(std::shared_ptr<Space> V, bool keep_diagonal,
+                                      int tile_threads = 0, int seg_cap_bytes = 0);
+// Re-cut the tiles of an existing plan (autotuning), re-uploading d_tiles.
+void retile(Pattern& P, int tile_threads, int seg_cap_bytes);
+
+// Launchers (kernels.cu).  All return after enqueueing on `stream`.
+struct FormArgs {
+  db2_form f;
+  const double* w = nullptr;   // device P1 field or null
+};
+void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int precision,
+                     double* vals, double* b, bool add_values, const uint8_t* bc_flags,
+                     const double* bc_vals, void* stream);
+void launch_apply(const Pattern& P, const FormArgs& a, int precision, const double* x, double* y,
+                  void* stream);
+void launch_vjp(const Pattern& P, const FormArgs& a, const FormArgs& L, int precision,
+                const double* gA, const double* gb, double* dkappa, double* scratch,
+                void* stream);
+void launch_expand_csr(const Pattern& P);
+void count_launch(int n = 1);
+void check_cuda(const char* what);
+size_t vjp_scratch_doubles(const Pattern& P);
+
+}  // namespace db2

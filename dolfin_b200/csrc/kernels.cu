@@ -1,0 +1,153 @@
+// kernels.cu -- launchers of the assembly, vector, action and adjoint kernels.
+#include <cuda_runtime.h>
+
+#include "launch.cuh"
+
+namespace db2 {
+
+namespace dev {
+
+// Vector-only assembly (Assembler::assemble for a rank-1 form): one thread
+// per dof (component c, node i) gathering its incident cells in cell order.
+template <int D, int P, int LOADM>
+__global__ void __launch_bounds__(256) k_assemble_vector(const AsmParams p, int bs) {
+  const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= p.nnodes * bs) return;
+  const int c = int(r / p.nnodes);
+  const int64_t node = r - int64_t(c) * p.nnodes;
+  double bsum = 0.0;
+  for (uint32_t ii = __ldg(p.inc_ptr + node); ii < __ldg(p.inc_ptr + node + 1); ++ii) {
+    const uint32_t word = __ldg(p.inc + ii);
+    const uint32_t cell = word & 0x0fffffffu;
+    const int li = int(word >> 28);
+    uint32_t pv[D + 1], code;
+    load_cell<D>(p, cell, li, pv, code);
+    double x[D + 1][D];
+    load_coords<D>(p, pv, x);
+    Geometry<D> G;
+    geometry(x, G);
+    double fv[D + 1];
+    if constexpr (LOADM == LOAD_P1)
+      for (int a = 0; a <= D; ++a) fv[a] = __ldg(p.f + pv[a]);
+    bsum += load_row<D, P, LOADM>(p, G, li <= D, c, fv);
+  }
+  double* bp = p.b + r;
+  *bp = p.add_values ? *bp + bsum : bsum;
+}
+
+}  // namespace dev
+
+dev::AsmParams make_params(const Pattern& P) {
+  const_cast<Pattern&>(P).ensure_device();
+  dev::AsmParams p{};
+  const Mesh& m = *P.V->mesh;
+  p.tiles = P.d_tiles.as<Tile>();
+  p.node_rowptr = P.d_node_rowptr.as<int32_t>();
+  p.inc_ptr = P.d_inc_ptr.as<uint32_t>();
+  p.inc = P.d_inc.as<uint32_t>();
+  p.pos = P.d_pos.as<uint8_t>();
+  p.cells = m.d_cells.as<uint32_t>();
+  p.x = m.d_x.as<double>();
+  p.cell_nodes = P.V->d_cell_nodes.as<uint32_t>();
+  p.cell_inc = P.d_cell_inc.as<uint32_t>();
+  p.kscale = 1.0;
+  p.fc[0] = p.fc[1] = p.fc[2] = 0.0;
+  p.nnz_node = P.nnz_node;
+  p.nnodes = P.V->nnodes;
+  return p;
+}
+
+// kappa of a bilinear form -> (uses P1 field, scale)
+static bool matrix_coeff(const FormArgs& a, dev::AsmParams& p) {
+  switch (a.f.coeff) {
+    case DB2_COEFF_NONE: p.kscale = 1.0; return false;
+    case DB2_COEFF_CONSTANT: p.kscale = a.f.constant[0]; return false;
+    case DB2_COEFF_P1:
+    case DB2_COEFF_P1_SCALED:
+      if (!a.w) fail(DB2_ERR_ARGUMENT, "form coefficient is a P1 Function but no field was given");
+      p.kappa = a.w;
+      p.kscale = a.f.coeff == DB2_COEFF_P1 ? 1.0 : a.f.constant[0];
+      return true;
+    default: fail(DB2_ERR_ARGUMENT, "unknown coefficient kind %d", a.f.coeff);
+  }
+}
+
+static int load_mode(const FormArgs* L, int bs, dev::AsmParams& p) {
+  if (!L) return dev::LOAD_NONE;
+  if (L->f.kind != DB2_FORM_LOAD) fail(DB2_ERR_ARGUMENT, "linear form must be DB2_FORM_LOAD");
+  switch (L->f.coeff) {
+    case DB2_COEFF_NONE:
+      for (int c = 0; c < 3; ++c) p.fc[c] = 1.0;
+      return dev::LOAD_CONST;
+    case DB2_COEFF_CONSTANT:
+      for (int c = 0; c < 3; ++c) p.fc[c] = bs == 1 ? L->f.constant[0] : L->f.constant[c];
+      return dev::LOAD_CONST;
+    case DB2_COEFF_P1:
+    case DB2_COEFF_P1_SCALED:
+      if (bs != 1) fail(DB2_ERR_UNSUPPORTED, "P1 load coefficient on a vector space");
+      if (!L->w) fail(DB2_ERR_ARGUMENT, "load coefficient is a P1 Function but no field was given");
+      p.f = L->w;
+      p.fc[0] = L->f.coeff == DB2_COEFF_P1 ? 1.0 : L->f.constant[0];
+      return dev::LOAD_P1;
+    default: fail(DB2_ERR_ARGUMENT, "unknown coefficient kind %d", L->f.coeff);
+  }
+}
+
+void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int precision,
+                     double* vals, double* b, bool add_values, const uint8_t* bc_flags,
+                     const double* bc_vals, void* stream) {
+  const Space& V = *P.V;
+  const int D = V.mesh->tdim;
+  dev::AsmParams p = make_params(P);
+  p.vals = vals;
+  p.b = b;
+  p.add_values = add_values ? 1 : 0;
+  p.bc_flags = bc_flags;
+  p.bc_vals = bc_vals;
+  const int loadm = load_mode(L, P.bs, p);
+  if (!a) {
+    // rank-1 form only
+    if (loadm == dev::LOAD_NONE) fail(DB2_ERR_ARGUMENT, "nothing to assemble");
+    const int64_t n = V.nnodes * P.bs;
+    const int threads = 256;
+    const unsigned blocks = unsigned((n + threads - 1) / threads);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+#define DB2_VEC(D_, P_)                                                                       \
+  if (D == D_ && V.degree == P_) {                                                            \
+    if (loadm == dev::LOAD_CONST) dev::k_assemble_vector<D_, P_, dev::LOAD_CONST><<<blocks, threads, 0, s>>>(p, P.bs); \
+    else dev::k_assemble_vector<D_, P_, dev::LOAD_P1><<<blocks, threads, 0, s>>>(p, P.bs);    \
+    count_launch();                                                                           \
+    check_cuda("assemble_vector launch");                                                     \
+    return;                                                                                   \
+  }
+    DB2_VEC(3, 1) DB2_VEC(3, 2) DB2_VEC(2, 1) DB2_VEC(2, 2)
+#undef DB2_VEC
+    fail(DB2_ERR_UNSUPPORTED, "vector assembly not provided for this element");
+  }
+  if (bc_flags) fail(DB2_ERR_UNSUPPORTED, "Dirichlet modification not provided by this kernel");
+  dev::LaunchCfg cfg;
+  cfg.ntiles = int(P.tiles.size());
+  cfg.threads = P.tile_threads;
+  cfg.smem = size_t(P.seg_cap) * sizeof(double);
+  cfg.stream = static_cast<cudaStream_t>(stream);
+  const bool fp32 = precision == DB2_FP32_CONTRACT;
+  if (precision != DB2_FP64 && precision != DB2_FP32_CONTRACT) fail(DB2_ERR_ARGUMENT, "unknown precision %d", precision);
+  bool ok = false;
+  if (a->f.kind == DB2_FORM_DIFFUSION) {
+    if (P.bs != 1) fail(DB2_ERR_UNSUPPORTED, "diffusion form on a vector space");
+    const bool kp1 = matrix_coeff(*a, p);
+    ok = D == 3 ? dev::dispatch_tet_diff(V.degree, p, cfg, kp1, loadm, fp32)
+                : dev::dispatch_tri_diff(V.degree, p, cfg, kp1, loadm, fp32);
+  } else if (a->f.kind == DB2_FORM_ELASTICITY) {
+    if (P.bs != D || D != 3) fail(DB2_ERR_UNSUPPORTED, "elasticity needs a 3D vector space");
+    p.mu = a->f.mu;
+    p.lmbda = a->f.lmbda;
+    if (a->f.coeff != DB2_COEFF_NONE) fail(DB2_ERR_UNSUPPORTED, "elasticity takes no coefficient");
+    ok = dev::dispatch_tet_elas(V.degree, p, cfg, false, loadm, fp32);
+  } else {
+    fail(DB2_ERR_ARGUMENT, "bilinear form kind %d not provided", a->f.kind);
+  }
+  if (!ok) fail(DB2_ERR_UNSUPPORTED, "no kernel for this form/coefficient/load combination");
+}
+
+}  // namespace db2

@@ -1,0 +1,64 @@
+// launch.cuh -- shared launch helpers for the assembly kernel instantiations.
+#pragma once
+
+#include "assemble.cuh"
+
+namespace db2 {
+namespace dev {
+
+struct LaunchCfg {
+  int ntiles;
+  int threads;
+  size_t smem;
+  cudaStream_t stream;
+};
+
+template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
+void run_assemble(const AsmParams& p, const LaunchCfg& cfg) {
+  auto kern = k_assemble<D, P, FORM, KP1, LOADM, CT>;
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    configured = true;
+  }
+  kern<<<cfg.ntiles, cfg.threads, cfg.smem, cfg.stream>>>(p);
+  count_launch();
+  check_cuda("assemble launch");
+}
+
+// Dispatch of the load mode / kappa / precision for one (D, P, FORM).
+template <int D, int P, int FORM>
+bool dispatch(const AsmParams& p, const LaunchCfg& cfg, bool kp1, int loadm, bool fp32) {
+#define DB2_RUN(KP1_, LM_)                                                               \
+  do {                                                                                   \
+    if (fp32) run_assemble<D, P, FORM, KP1_, LM_, float>(p, cfg);                         \
+    else run_assemble<D, P, FORM, KP1_, LM_, double>(p, cfg);                             \
+    return true;                                                                         \
+  } while (0)
+  if constexpr (FORM == FORM_ELAS) {
+    if (kp1) return false;
+    if (loadm == LOAD_NONE) DB2_RUN(false, LOAD_NONE);
+    if (loadm == LOAD_CONST) DB2_RUN(false, LOAD_CONST);
+    return false;
+  } else {
+    if (kp1) {
+      if (loadm == LOAD_NONE) DB2_RUN(true, LOAD_NONE);
+      if (loadm == LOAD_CONST) DB2_RUN(true, LOAD_CONST);
+      if (loadm == LOAD_P1) DB2_RUN(true, LOAD_P1);
+    } else {
+      if (loadm == LOAD_NONE) DB2_RUN(false, LOAD_NONE);
+      if (loadm == LOAD_CONST) DB2_RUN(false, LOAD_CONST);
+      if (loadm == LOAD_P1) DB2_RUN(false, LOAD_P1);
+    }
+    return false;
+  }
+#undef DB2_RUN
+}
+
+// Per-translation-unit entry points (assemble_*.cu).
+bool dispatch_tet_diff(int P, const AsmParams& p, const LaunchCfg& cfg, bool kp1, int loadm, bool fp32);
+bool dispatch_tri_diff(int P, const AsmParams& p, const LaunchCfg& cfg, bool kp1, int loadm, bool fp32);
+bool dispatch_tet_elas(int P, const AsmParams& p, const LaunchCfg& cfg, bool kp1, int loadm, bool fp32);
+
+}  // namespace dev
+}  // namespace db2

@@ -1,0 +1,193 @@
+/*
+ * dolfin_b200.h -- C ABI of the B200 finite-element assembly engine.
+ *
+ * The engine replaces the hot path of DOLFIN 2019.1 assembly
+ * (dolfin::Assembler / SystemAssembler and Python dolfin.assemble) for the
+ * named Lagrange forms on simplices.  Host structures (mesh, dofmap,
+ * sparsity pattern) are built on the CPU exactly as DOLFIN builds them with
+ * parameters["reorder_dofs_serial"] = False and uploaded once; assembly runs
+ * as hand-written sm_100a kernels on caller-provided device buffers.
+ *
+ * Conventions
+ *   - every entry point returns DB2_OK (0) or a DB2_ERR_* code; the message
+ *     of the last failure on the calling thread is db2_last_error().  This
+ *     replaces dolfin_error() (dolfin/log/log.cpp:129), which throws.
+ *   - pointers documented as "device" are CUDA global-memory pointers on the
+ *     current device; "host" pointers are ordinary CPU memory.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream); all device work of a call is ordered on it and the call does
+ *     not synchronise unless stated.
+ *   - objects are owned by the caller and released with *_destroy; a space
+ *     keeps its mesh alive and a pattern keeps its space alive by reference
+ *     (destroy in reverse order of creation).
+ */
+#ifndef DOLFIN_B200_H
+#define DOLFIN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ----------------------------------------------------- */
+#define DB2_OK 0
+#define DB2_ERR_ARGUMENT 1    /* NULL or out-of-range argument               */
+#define DB2_ERR_SHAPE 2       /* dimensions do not match the form/space      */
+#define DB2_ERR_INDEX 3       /* vertex/dof index out of range               */
+#define DB2_ERR_MESH 4        /* mesh not ordered / degenerate cell          */
+#define DB2_ERR_UNSUPPORTED 5 /* element/form combination not provided       */
+#define DB2_ERR_CUDA 6        /* CUDA runtime error                          */
+#define DB2_ERR_NOMEM 7       /* host or device allocation failed            */
+#define DB2_ERR_TIMEOUT 8     /* bounded device wait ran out                 */
+
+/* ---- opaque handles --------------------------------------------------- */
+typedef struct db2_mesh_t* db2_mesh;
+typedef struct db2_space_t* db2_space;
+typedef struct db2_pattern_t* db2_pattern;
+typedef struct db2_batch_t* db2_batch;
+
+/* ---- forms ------------------------------------------------------------ */
+enum db2_form_kind {
+  DB2_FORM_DIFFUSION = 1,  /* a = kappa*inner(grad(u), grad(v))*dx          */
+  DB2_FORM_LOAD = 2,       /* L = f*v*dx (scalar), inner(f, v)*dx (vector)  */
+  DB2_FORM_ELASTICITY = 3  /* a = inner(sigma(u), epsilon(v))*dx,
+                              sigma = 2 mu epsilon + lmbda tr(epsilon) I    */
+};
+enum db2_coeff_kind {
+  DB2_COEFF_NONE = 0,      /* coefficient 1                                 */
+  DB2_COEFF_CONSTANT = 1,  /* dolfin Constant: constant[] (scalar or vector)*/
+  DB2_COEFF_P1 = 2,        /* P1 Function: device array of vertex values     */
+  DB2_COEFF_P1_SCALED = 3  /* constant[0] * P1 Function                      */
+};
+enum db2_precision {
+  DB2_FP64 = 0,            /* geometry, contraction, accumulation in FP64    */
+  DB2_FP32_CONTRACT = 1    /* FP64 geometry and global accumulation; the
+                              reference-tensor contraction in FP32           */
+};
+
+typedef struct {
+  int kind;            /* db2_form_kind                                     */
+  int coeff;           /* db2_coeff_kind of kappa (a) or f (L)              */
+  double constant[3];  /* constant value(s)                                 */
+  double mu, lmbda;    /* elasticity Lame constants                         */
+} db2_form;
+
+/* ---- library ---------------------------------------------------------- */
+const char* db2_last_error(void);
+const char* db2_version(void);
+/* Number of engine kernels launched by this process so far (all streams). */
+int64_t db2_kernel_launches(void);
+
+/* ---- mesh (dolfin::Mesh, dolfin/mesh/Mesh.h; MeshGeometry/MeshTopology) */
+/* Mesh from host arrays: coords[nv*tdim] (gdim == tdim), cells[nc*(tdim+1)].
+   Each cell's vertex list must be sorted ascending (an ordered mesh,
+   DofMapBuilder.cpp:62-68 rejects unordered meshes); replaces
+   MeshEditor::open/add_vertex/add_cell/close (dolfin/mesh/MeshEditor.h). */
+int db2_mesh_create(int tdim, int64_t nv, const double* coords, int64_t nc,
+                    const uint32_t* cells, db2_mesh* out);
+/* UnitCubeMesh(nx,ny,nz): BoxMesh::build_tet (dolfin/generation/BoxMesh.cpp:50-170). */
+int db2_mesh_unit_cube(int nx, int ny, int nz, db2_mesh* out);
+/* UnitSquareMesh(nx,ny,diagonal): RectangleMesh::build_tri
+   (dolfin/generation/RectangleMesh.cpp:46-233); diagonal 0 "right", 1 "left",
+   2 "right/left", 3 "left/right". */
+int db2_mesh_unit_square(int nx, int ny, int diagonal, db2_mesh* out);
+int db2_mesh_info(db2_mesh m, int* tdim, int64_t* nv, int64_t* nc);
+/* Host copies of Mesh::coordinates() and Mesh::cells(). */
+int db2_mesh_copy(db2_mesh m, double* coords, uint32_t* cells);
+/* Overwrite vertex coordinates (host array nv*tdim); topology unchanged. */
+int db2_mesh_set_coordinates(db2_mesh m, const double* coords);
+/* Number of edges (mesh.init(1); TopologyComputation key matching). */
+int db2_mesh_num_edges(db2_mesh m, int64_t* ne);
+int db2_mesh_destroy(db2_mesh m);
+
+/* ---- function space + dofmap (DofMap, DofMapBuilder::build) ----------- */
+/* Continuous Lagrange P1/P2 with value_size 1 or tdim; natural UFC
+   numbering (DofMapBuilder.cpp:253-272), vector spaces component-major. */
+int db2_space_create(db2_mesh m, int degree, int value_size, db2_space* out);
+int db2_space_info(db2_space V, int* ndofs_per_cell, int64_t* dim);
+/* DofMap::cell_dofs for all cells (dolfin/fem/DofMap.h:201-206), host out[nc*ndofs]. */
+int db2_space_cell_dofs(db2_space V, int32_t* out);
+int db2_space_destroy(db2_space V);
+
+/* ---- sparsity pattern + assembly plan --------------------------------- */
+/* SparsityPatternBuilder::build (dolfin/fem/SparsityPatternBuilder.cpp:42-269)
+   + EigenMatrix::init (dolfin/la/EigenMatrix.cpp:384-410) for a on V x V:
+   sorted CSR (int32 rowptr/cols, as Eigen::SparseMatrix<double,RowMajor,int>),
+   plus the engine's row-gather plan.  keep_diagonal as AssemblerBase.h:67. */
+int db2_pattern_create(db2_space V, int keep_diagonal, db2_pattern* out);
+int db2_pattern_info(db2_pattern P, int64_t* nrows, int64_t* nnz);
+/* Device CSR arrays owned by the pattern (EigenMatrix::data(),
+   dolfin/la/EigenMatrix.h:193-194). */
+int db2_pattern_csr_device(db2_pattern P, const int32_t** rowptr, const int32_t** cols);
+/* Host copies: rowptr[nrows+1], cols[nnz]. */
+int db2_pattern_csr_host(db2_pattern P, int32_t* rowptr, int32_t* cols);
+int db2_pattern_destroy(db2_pattern P);
+/* Diagnostics of the row-gather plan (no reference counterpart; used by the
+   tests and the autotuner): node-level graph, node -> (cell | local node<<28)
+   incidences in cell order, per-incidence column slots (kp bytes each), and
+   tiles as int32 quadruples (component, first node, end node, 0). */
+int db2_pattern_plan_info(db2_pattern P, int64_t* nnodes, int64_t* nincidences, int* kp,
+                          int64_t* ntiles);
+int db2_pattern_plan_copy(db2_pattern P, int32_t* node_rowptr, int32_t* node_cols,
+                          uint32_t* inc_ptr, uint32_t* inc, uint8_t* pos, int32_t* tiles);
+/* Re-cut the pattern's tiles: at most tile_threads row units per CTA and
+   seg_cap_bytes of shared-memory row segment. */
+int db2_pattern_retile(db2_pattern P, int tile_threads, int seg_cap_bytes);
+
+/* ---- assembly --------------------------------------------------------- */
+/* Assembler::assemble(A, a) (dolfin/fem/Assembler.cpp:52-103) for a bilinear
+   form on the pattern's space: writes CSR values vals[nnz] (device).  w is
+   the device P1 coefficient (kappa) when a.coeff is P1/P1_SCALED.
+   add_values as AssemblerBase.h:46 (accumulate into vals). */
+int db2_assemble_matrix(db2_pattern P, const db2_form* a, const double* w, int precision,
+                        double* vals, int add_values, void* stream);
+/* Assembler::assemble(b, L) for a linear form: b[N] (device). */
+int db2_assemble_vector(db2_pattern P, const db2_form* L, const double* w, double* b,
+                        int add_values, void* stream);
+/* SystemAssembler(a, L).assemble(A, b) (dolfin/fem/SystemAssembler.cpp:138-301,
+   cell_wise_assembly :303-492) without boundary conditions: A and b in one
+   pass sharing the geometry of each cell. */
+int db2_assemble_system(db2_pattern P, const db2_form* a, const double* wa, const db2_form* L,
+                        const double* wL, int precision, double* vals, double* b, void* stream);
+/* SystemAssembler with DirichletBC: symmetric modification
+   SystemAssembler::apply_bc (dolfin/fem/SystemAssembler.cpp:1037-1070) in the
+   element epilogue.  bc_flags[N] (device, uint8: 1 = Dirichlet dof) and
+   bc_vals[N] (device). */
+int db2_assemble_system_bc(db2_pattern P, const db2_form* a, const double* wa, const db2_form* L,
+                           const double* wL, const uint8_t* bc_flags, const double* bc_vals,
+                           int precision, double* vals, double* b, void* stream);
+/* Matrix-free action y = A(a) x (device x[N], y[N]); replaces assembling A
+   and calling GenericMatrix::mult (dolfin/la/GenericMatrix.h). */
+int db2_apply(db2_pattern P, const db2_form* a, const double* w, int precision, const double* x,
+              double* y, void* stream);
+/* Vector-Jacobian product of (A(kappa), b(kappa)) for a = kappa grad.grad
+   (P1 kappa) and L = f v dx, or kappa f v dx when L->coeff is
+   DB2_COEFF_P1_SCALED with constant[0] ignored: dkappa[Nv] = sum gA*dA/dkappa
+   + sum gb*db/dkappa.  gA[nnz], gb[N] device (gb may be NULL).  This is the
+   assembly of UFL's derivative(a, kappa) form (the reference's
+   python/test/unit/fem/test_coordinate_derivative.py style check). */
+int db2_vjp_kappa(db2_pattern P, const db2_form* a, const double* kappa, const db2_form* L,
+                  const double* f, const double* gA, const double* gb, int precision,
+                  double* dkappa, void* stream);
+
+/* ---- batched multi-mesh assembly -------------------------------------- */
+/* A batch of patterns (any element/space mix) assembled by ONE persistent
+   launch.  kappa pointers (device, one P1 field per member) and output
+   pointers are fixed at creation so that the launch can be captured in a
+   CUDA graph.  tile_nodes/seg_cap_bytes/ctas_per_sm = 0 choose defaults
+   (the autotuner in dolfin_b200.batch chooses explicit values). */
+int db2_batch_create(int count, const db2_pattern* patterns, const db2_form* forms,
+                     const double* const* kappas, double* const* vals,
+                     int tile_nodes, int seg_cap_bytes, int ctas_per_sm, db2_batch* out);
+int db2_batch_info(db2_batch B, int64_t* tiles, int64_t* cells, int* ctas);
+/* One persistent launch over every tile of every member (precision as above). */
+int db2_batch_assemble(db2_batch B, int precision, void* stream);
+/* Reference path: one launch per member, in member order. */
+int db2_batch_assemble_loop(db2_batch B, int precision, void* stream);
+int db2_batch_destroy(db2_batch B);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DOLFIN_B200_H */
