@@ -59,7 +59,8 @@ _SIGS = {
     "db2_pattern_info": [P, C.POINTER(I64), C.POINTER(I64)],
     "db2_pattern_csr_device": [P, PP, PP],
     "db2_pattern_csr_host": [P, P, P],
-    "db2_pattern_plan_info": [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I), C.POINTER(I64)],
+    "db2_pattern_plan_info": [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I), C.POINTER(I64),
+                              C.POINTER(I64), C.POINTER(I64)],
     "db2_pattern_plan_copy": [P, P, P, P, P, P, P],
     "db2_pattern_retile": [P, I, I],
     "db2_pattern_destroy": [P],

@@ -250,8 +250,11 @@ class SparsityPattern(_Handle):
 
     def plan(self):
         nn, ninc, kp, nt = C.c_int64(), C.c_int64(), C.c_int(), C.c_int64()
-        call("db2_pattern_plan_info", self._h, C.byref(nn), C.byref(ninc), C.byref(kp), C.byref(nt))
+        ng, ntyp = C.c_int64(), C.c_int64()
+        call("db2_pattern_plan_info", self._h, C.byref(nn), C.byref(ninc), C.byref(kp), C.byref(nt),
+             C.byref(ng), C.byref(ntyp))
         nn, ninc, kp, nt = nn.value, ninc.value, kp.value, nt.value
+        self.ngroups, self.ntypes = ng.value, ntyp.value
         node_rowptr = np.empty(nn + 1, np.int32)
         rp = node_rowptr
         call("db2_pattern_plan_copy", self._h, _ptr(rp), None, None, None, None, None)
@@ -266,6 +269,7 @@ class SparsityPattern(_Handle):
                     pos=pos.reshape(ninc, kp), tiles=tiles, kp=kp)
 
     def retile(self, tile_threads, seg_cap_bytes):
+        """Launch shape of the assembly kernel (see db2_pattern_retile)."""
         call("db2_pattern_retile", self._h, int(tile_threads), int(seg_cap_bytes))
 
 

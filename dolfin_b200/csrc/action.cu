@@ -54,16 +54,15 @@ __global__ void __launch_bounds__(256) k_apply(const AsmParams p, const double* 
   const int64_t node = r - int64_t(c) * p.nnodes;
   double acc = 0.0;
   for (uint32_t ii = __ldg(p.inc_ptr + node); ii < __ldg(p.inc_ptr + node + 1); ++ii) {
-    const uint32_t word = __ldg(p.inc + ii);
+    const uint32_t word = rec_word<D, P>(p, ii);
     const uint32_t cell = word & 0x0fffffffu;
     const int li = int(word >> 28);
-    uint32_t pv[D + 1], code;
-    load_cell<D>(p, cell, li, pv, code);
-    double x[D + 1][D];
-    load_coords<D>(p, pv, x);
-    double kap[D + 1];
-    if constexpr (KP1)
-      for (int a = 0; a <= D; ++a) kap[a] = __ldg(p.kappa + pv[a]);
+    const uint32_t code = perm_of<D>(li);
+    uint32_t v[D + 1], pv[D + 1];
+    load_verts<D>(p, cell, v);
+    relabel<D>(v, code, pv);
+    double x[D + 1][D], kap[D + 1], fv[D + 1];
+    load_vertex_data<D, false>(p, pv, x, kap, fv);
     Geometry<D> G;
     geometry(x, G);
     uint32_t nodes[E::K];
@@ -100,27 +99,25 @@ __global__ void __launch_bounds__(256) k_vjp_cells(const AsmParams p, int64_t nc
     const uint32_t ii = __ldg(p.cell_inc + size_t(cell) * E::K + li);
     const uint32_t node = __ldg(cn + li);
     const double* grow = gA + __ldg(p.node_rowptr + node);
-    uint32_t pv[D + 1], code;
-    load_cell<D>(p, uint32_t(cell), li, pv, code);
-    double x[D + 1][D];
-    load_coords<D>(p, pv, x);
+    const uint32_t code = perm_of<D>(li);
+    uint32_t v[D + 1], pv[D + 1];
+    load_verts<D>(p, uint32_t(cell), v);
+    relabel<D>(v, code, pv);
+    double x[D + 1][D], kap_unused[D + 1], f_unused[D + 1];
+    load_vertex_data<D, false>(p, pv, x, kap_unused, f_unused);
     Geometry<D> G;
     geometry(x, G);
     const bool vertex = li <= D;
     // gA at the row's slots, in the relabelled local order
-    const uint32_t* pw = reinterpret_cast<const uint32_t*>(p.pos + size_t(ii) * E::KP);
     double g[E::K];
-    for (int q = 0; q < E::KP / 4; ++q) {
-      const uint32_t w = __ldg(pw + q);
-      for (int s = 0; s < 4; ++s)
-        if (4 * q + s < E::K) g[4 * q + s] = __ldg(grow + ((w >> (8 * s)) & 0xffu));
-    }
+#pragma unroll
+    for (int j = 0; j < E::K; ++j) g[j] = __ldg(grow + rec_slot<D, P>(p, ii, j));
     CT W0[1][NB];
     CT W1[2][NB];
-    for (int b = 0; b < NB; ++b) W0[0][b] = CT(G.vol * gdot<D>(G, 0, b) * p.kscale);
+    for (int b = 0; b < NB; ++b) W0[0][b] = CT(ndot<D>(G, 0, b) * (G.s * p.kscale));
     if constexpr (P == 2)
       for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < NB; ++b) W1[a][b] = CT(G.vol * gdot<D>(G, a, b) * p.kscale);
+        for (int b = 0; b < NB; ++b) W1[a][b] = CT(ndot<D>(G, a, b) * (G.s * p.kscale));
     double fv[NB];
     if constexpr (LOADK)
       for (int a = 0; a < NB; ++a) fv[a] = __ldg(p.f + pv[a]);
@@ -156,7 +153,7 @@ __global__ void __launch_bounds__(256) k_vjp_cells(const AsmParams p, int64_t nc
 
 // Adjoint, step 2 (one thread per vertex): dkappa[v] = sum over cells around
 // v, in cell order, of t[cell][local index of v].
-template <int D>
+template <int D, int P>
 __global__ void __launch_bounds__(256) k_vjp_vertices(const AsmParams p, int64_t nv,
                                                       const double* __restrict__ t,
                                                       double* __restrict__ dk) {
@@ -164,7 +161,7 @@ __global__ void __launch_bounds__(256) k_vjp_vertices(const AsmParams p, int64_t
   if (v >= nv) return;
   double s = 0.0;
   for (uint32_t ii = __ldg(p.inc_ptr + v); ii < __ldg(p.inc_ptr + v + 1); ++ii) {
-    const uint32_t word = __ldg(p.inc + ii);
+    const uint32_t word = rec_word<D, P>(p, ii);
     s += __ldg(t + size_t(word & 0x0fffffffu) * (D + 1) + (word >> 28));
   }
   dk[v] = s;
@@ -181,6 +178,7 @@ void run_apply(const AsmParams& p, int bs, const double* x, double* y, cudaStrea
 }  // namespace dev
 
 dev::AsmParams make_params(const Pattern& P);
+void pack_vertex_records(const Pattern& P, const double* kappa, const double* f, void* stream);
 
 void launch_apply(const Pattern& P, const FormArgs& a, int precision, const double* x, double* y,
                   void* stream) {
@@ -196,6 +194,7 @@ void launch_apply(const Pattern& P, const FormArgs& a, int precision, const doub
     kp1 = a.f.coeff == DB2_COEFF_P1 || a.f.coeff == DB2_COEFF_P1_SCALED;
     if (kp1 && !a.w) fail(DB2_ERR_ARGUMENT, "P1 coefficient field missing");
     p.kappa = a.w;
+    pack_vertex_records(P, kp1 ? a.w : nullptr, nullptr, stream);
 #define DB2_AP(D_, P_)                                                                  \
   if (D == D_ && deg == P_) {                                                           \
     if (kp1) {                                                                          \
@@ -262,7 +261,7 @@ void launch_vjp(const Pattern& P, const FormArgs& a, const FormArgs& L, int prec
       if (fp32) dev::k_vjp_cells<D_, P_, false, float><<<bc, 256, 0, s>>>(p, nc, gA, gb, scratch); \
       else dev::k_vjp_cells<D_, P_, false, double><<<bc, 256, 0, s>>>(p, nc, gA, gb, scratch); \
     }                                                                                          \
-    dev::k_vjp_vertices<D_><<<bv, 256, 0, s>>>(p, nv, scratch, dkappa);                         \
+    dev::k_vjp_vertices<D_, P_><<<bv, 256, 0, s>>>(p, nv, scratch, dkappa);                         \
     count_launch(2);                                                                           \
     check_cuda("vjp launch");                                                                  \
     return;                                                                                    \

@@ -14,6 +14,8 @@
 //     tensor x geometry tensor, and adds it into its own row segment at the
 //     precomputed column slots.  Rows never share slots, so the scatter is
 //     deterministic without atomics.
+//   * the loads of an incidence (record -> cell vertices -> vertex records)
+//     are software-pipelined two incidences ahead of the arithmetic.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -34,7 +36,8 @@ struct El {
   static constexpr int NV = D + 1;
   static constexpr int NE = D == 3 ? 6 : 3;
   static constexpr int K = P == 1 ? NV : NV + NE;
-  static constexpr int KP = (K + 3) / 4 * 4;
+  // incidence record: u32 word (cell | local node << 28), then K slot bytes
+  static constexpr int RS = 4 + K <= 8 ? 8 : 16;
 };
 
 // ---- canonical relabelling ----------------------------------------------
@@ -98,55 +101,60 @@ __device__ __forceinline__ T sel3(const T (&v)[3], uint32_t idx) {
 }
 
 // ---- geometry (FP64) ------------------------------------------------------
-// Barycentric gradients g[a] = grad(lambda_a) and |T| of the affine simplex
-// with (relabelled) vertices x[0..D]: rows of J^-1 for a >= 1, g[0] = -sum.
+// For the affine simplex with (relabelled) vertices x[0..D]: the unnormalised
+// barycentric gradients n[a] = det(J) * grad(lambda_a) (cofactor vectors of
+// J = [x1-x0, x2-x0, ...], n[0] = -sum), s = 1 / (D! |det J|) and |T|.
+// Then |T| grad(l_a).grad(l_b) = s * n[a].n[b]: the geometry tensor needs one
+// reciprocal and no division of the gradients.
 template <int D>
 struct Geometry {
-  double g[D + 1][D];
+  double n[D + 1][D];
+  double s;
   double vol;
 };
 
 __device__ __forceinline__ void geometry(const double (&x)[4][3], Geometry<3>& G) {
   double c[3][3];
+#pragma unroll
   for (int m = 0; m < 3; ++m)
+#pragma unroll
     for (int r = 0; r < 3; ++r) c[m][r] = x[m + 1][r] - x[0][r];
-  double n[3][3];  // n[m] = c[m+1] x c[m+2]
-  for (int m = 0; m < 3; ++m) {
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {  // n[m+1] = c[m+1] x c[m+2]
     const double* a = c[(m + 1) % 3];
     const double* b = c[(m + 2) % 3];
-    n[m][0] = a[1] * b[2] - a[2] * b[1];
-    n[m][1] = a[2] * b[0] - a[0] * b[2];
-    n[m][2] = a[0] * b[1] - a[1] * b[0];
+    G.n[m + 1][0] = a[1] * b[2] - a[2] * b[1];
+    G.n[m + 1][1] = a[2] * b[0] - a[0] * b[2];
+    G.n[m + 1][2] = a[0] * b[1] - a[1] * b[0];
   }
-  const double det = c[0][0] * n[0][0] + c[0][1] * n[0][1] + c[0][2] * n[0][2];
-  const double inv = __drcp_rn(det);
-  for (int r = 0; r < 3; ++r) {
-    G.g[1][r] = n[0][r] * inv;
-    G.g[2][r] = n[1][r] * inv;
-    G.g[3][r] = n[2][r] * inv;
-    G.g[0][r] = -(G.g[1][r] + G.g[2][r] + G.g[3][r]);
-  }
-  G.vol = fabs(det) * (1.0 / 6.0);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) G.n[0][r] = -(G.n[1][r] + G.n[2][r] + G.n[3][r]);
+  const double det = c[0][0] * G.n[1][0] + c[0][1] * G.n[1][1] + c[0][2] * G.n[1][2];
+  const double ad = fabs(det);
+  G.vol = ad * (1.0 / 6.0);
+  G.s = __drcp_rn(6.0 * ad);
 }
 
 __device__ __forceinline__ void geometry(const double (&x)[3][2], Geometry<2>& G) {
   const double c1x = x[1][0] - x[0][0], c1y = x[1][1] - x[0][1];
   const double c2x = x[2][0] - x[0][0], c2y = x[2][1] - x[0][1];
   const double det = c1x * c2y - c1y * c2x;
-  const double inv = __drcp_rn(det);
-  G.g[1][0] = c2y * inv;
-  G.g[1][1] = -c2x * inv;
-  G.g[2][0] = -c1y * inv;
-  G.g[2][1] = c1x * inv;
-  G.g[0][0] = -(G.g[1][0] + G.g[2][0]);
-  G.g[0][1] = -(G.g[1][1] + G.g[2][1]);
-  G.vol = fabs(det) * 0.5;
+  G.n[1][0] = c2y;
+  G.n[1][1] = -c2x;
+  G.n[2][0] = -c1y;
+  G.n[2][1] = c1x;
+  G.n[0][0] = -(c2y - c1y);
+  G.n[0][1] = -(c1x - c2x);
+  const double ad = fabs(det);
+  G.vol = ad * 0.5;
+  G.s = __drcp_rn(2.0 * ad);
 }
 
 template <int D>
-__device__ __forceinline__ double gdot(const Geometry<D>& G, int a, int b) {
-  double s = G.g[a][0] * G.g[b][0];
-  for (int r = 1; r < D; ++r) s = fma(G.g[a][r], G.g[b][r], s);
+__device__ __forceinline__ double ndot(const Geometry<D>& G, int a, int b) {
+  double s = G.n[a][0] * G.n[b][0];
+#pragma unroll
+  for (int r = 1; r < D; ++r) s = fma(G.n[a][r], G.n[b][r], s);
   return s;
 }
 
@@ -202,15 +210,14 @@ struct AsmParams {
   const Tile* tiles;
   const int32_t* node_rowptr;
   const uint32_t* inc_ptr;
-  const uint32_t* inc;
-  const uint8_t* pos;
+  const unsigned char* rec;  // incidence records (El::RS bytes each)
   const uint32_t* cells;
-  const double* x;          // padded coordinates
+  const double* xw;          // vertex records: 3D (x,y,z,kappa), 2D (x,y,kappa,f)
   const uint32_t* cell_nodes;
-  const uint32_t* cell_inc; // incidence index of (cell, local node)
-  const double* kappa;      // P1 field (matrix form) or null
+  const uint32_t* cell_inc;  // incidence index of (cell, local node)
+  const double* kappa;       // P1 field (matrix form) or null
   double kscale;
-  const double* f;          // P1 field (load form) or null
+  const double* f;           // P1 field (load form) or null
   double fc[3];
   double mu, lmbda;
   double* vals;
@@ -218,50 +225,74 @@ struct AsmParams {
   int64_t nnz_node;
   int64_t nnodes;
   int add_values;
-  const uint8_t* bc_flags;  // dof-level Dirichlet flags or null
+  const uint8_t* bc_flags;   // dof-level Dirichlet flags or null
   const double* bc_vals;
 };
 
-// Loads the relabelled vertices of cell `cell` for local node li.
+template <int D, int P>
+__device__ __forceinline__ uint32_t rec_word(const AsmParams& p, uint32_t ii) {
+  return __ldg(reinterpret_cast<const uint32_t*>(p.rec + size_t(ii) * El<D, P>::RS));
+}
+template <int D, int P>
+__device__ __forceinline__ uint32_t rec_slot(const AsmParams& p, uint32_t ii, int j) {
+  return __ldg(p.rec + size_t(ii) * El<D, P>::RS + 4 + j);
+}
+
+// Relabelled vertex ids of a cell for local node li (vertex ids v[] as stored).
 template <int D>
-__device__ __forceinline__ void load_cell(const AsmParams& p, uint32_t cell, int li,
-                                          uint32_t (&pv)[D + 1], uint32_t& code) {
-  code = perm_of<D>(li);
-  if constexpr (D == 3) {
-    const uint4 v4 = __ldg(reinterpret_cast<const uint4*>(p.cells) + cell);
-    const uint32_t v[4] = {v4.x, v4.y, v4.z, v4.w};
-    for (int a = 0; a < 4; ++a) pv[a] = sel4(v, (code >> (2 * a)) & 3u);
-  } else {
-    const uint32_t* c = p.cells + 3 * size_t(cell);
-    const uint32_t v[3] = {__ldg(c), __ldg(c + 1), __ldg(c + 2)};
-    for (int a = 0; a < 3; ++a) pv[a] = sel3(v, (code >> (2 * a)) & 3u);
+__device__ __forceinline__ void relabel(const uint32_t (&v)[D + 1], uint32_t code,
+                                        uint32_t (&pv)[D + 1]) {
+#pragma unroll
+  for (int a = 0; a <= D; ++a) {
+    const uint32_t k = (code >> (2 * a)) & 3u;
+    if constexpr (D == 3) pv[a] = sel4(v, k);
+    else pv[a] = sel3(v, k);
   }
 }
 
 template <int D>
-__device__ __forceinline__ void load_coords(const AsmParams& p, const uint32_t (&pv)[D + 1],
-                                            double (&x)[D + 1][D]) {
+__device__ __forceinline__ void load_verts(const AsmParams& p, uint32_t cell, uint32_t (&v)[D + 1]) {
   if constexpr (D == 3) {
-    const double2* X = reinterpret_cast<const double2*>(p.x);
-    for (int a = 0; a < 4; ++a) {
-      const double2 xy = __ldg(X + 2 * size_t(pv[a]));
-      const double2 zw = __ldg(X + 2 * size_t(pv[a]) + 1);
-      x[a][0] = xy.x;
-      x[a][1] = xy.y;
-      x[a][2] = zw.x;
-    }
+    const uint4 v4 = __ldg(reinterpret_cast<const uint4*>(p.cells) + cell);
+    v[0] = v4.x; v[1] = v4.y; v[2] = v4.z; v[3] = v4.w;
   } else {
-    const double2* X = reinterpret_cast<const double2*>(p.x);
-    for (int a = 0; a < 3; ++a) {
-      const double2 xy = __ldg(X + pv[a]);
-      x[a][0] = xy.x;
-      x[a][1] = xy.y;
+    const uint32_t* c = p.cells + 3 * size_t(cell);
+    v[0] = __ldg(c); v[1] = __ldg(c + 1); v[2] = __ldg(c + 2);
+  }
+}
+
+// One 256-bit read-only load of a vertex record.
+__device__ __forceinline__ void ld_rec4(const double* ptr, double& a, double& b, double& c, double& d) {
+  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(a), "=d"(b), "=d"(c), "=d"(d)
+               : "l"(ptr));
+}
+
+// Loads the relabelled cell's coordinates (and kappa, f from the vertex records).
+template <int D, bool FP1>
+__device__ __forceinline__ void load_vertex_data(const AsmParams& p, const uint32_t (&pv)[D + 1],
+                                                 double (&x)[D + 1][D], double (&kap)[D + 1],
+                                                 double (&fv)[D + 1]) {
+#pragma unroll
+  for (int a = 0; a <= D; ++a) {
+    double r0, r1, r2, r3;
+    ld_rec4(p.xw + 4 * size_t(pv[a]), r0, r1, r2, r3);
+    if constexpr (D == 3) {
+      x[a][0] = r0; x[a][1] = r1; x[a][2] = r2;
+      kap[a] = r3;
+      if constexpr (FP1) fv[a] = __ldg(p.f + pv[a]);
+    } else {
+      x[a][0] = r0; x[a][1] = r1;
+      kap[a] = r2;
+      fv[a] = r3;
     }
   }
 }
 
 // Element-matrix row of the canonical node (vertex 0 or edge (0,1)) for the
-// trial component block e (test component c) into out[K] (contraction type CT).
+// trial component block e (test component c) into out[K] (contraction type CT):
+// the FP64 geometry tensor W is formed, rounded to CT, and contracted with the
+// generated reference tensor in CT.
 template <int D, int P, int FORM, bool KP1, typename CT>
 __device__ __forceinline__ void element_row(const AsmParams& p, const Geometry<D>& G,
                                             bool vertex, int c, int e,
@@ -270,31 +301,37 @@ __device__ __forceinline__ void element_row(const AsmParams& p, const Geometry<D
   using R = Rows<D, P, CT>;
   constexpr int NB = D + 1;
   CT kc[NB];
-  if constexpr (KP1)
+  if constexpr (KP1) {
+#pragma unroll
     for (int a = 0; a < NB; ++a) kc[a] = CT(kap[a]);
+  }
   auto wval = [&](int a, int b) -> double {
     if constexpr (FORM == FORM_DIFF) {
-      return G.vol * gdot<D>(G, a, b) * p.kscale;
+      return ndot<D>(G, a, b) * (G.s * p.kscale);
     } else {
-      double gac = G.g[a][0], gae = G.g[a][0], gbc = G.g[b][0], gbe = G.g[b][0];
+      double nac = G.n[a][0], nae = G.n[a][0], nbc = G.n[b][0], nbe = G.n[b][0];
+#pragma unroll
       for (int r = 1; r < D; ++r) {
-        if (c == r) { gac = G.g[a][r]; gbc = G.g[b][r]; }
-        if (e == r) { gae = G.g[a][r]; gbe = G.g[b][r]; }
+        if (c == r) { nac = G.n[a][r]; nbc = G.n[b][r]; }
+        if (e == r) { nae = G.n[a][r]; nbe = G.n[b][r]; }
       }
-      double w = p.lmbda * gac * gbe + p.mu * gae * gbc;
-      if (c == e) w = fma(p.mu, gdot<D>(G, a, b), w);
-      return G.vol * w;
+      double w = p.lmbda * nac * nbe + p.mu * nae * nbc;
+      if (c == e) w = fma(p.mu, ndot<D>(G, a, b), w);
+      return G.s * w;
     }
   };
   if (P == 1 || vertex) {
     CT W[1][NB];
+#pragma unroll
     for (int b = 0; b < NB; ++b) W[0][b] = CT(wval(0, b));
     if constexpr (KP1) R::v_kp1(W, kc, out);
     else R::v_k1(W, out);
   } else {
     if constexpr (P == 2) {
       CT W[2][NB];
+#pragma unroll
       for (int a = 0; a < 2; ++a)
+#pragma unroll
         for (int b = 0; b < NB; ++b) W[a][b] = CT(wval(a, b));
       if constexpr (KP1) R::e_kp1(W, kc, out);
       else R::e_k1(W, out);
@@ -321,12 +358,64 @@ __device__ __forceinline__ double load_row(const AsmParams& p, const Geometry<D>
   }
 }
 
+// ---- incidence fetch pipeline ---------------------------------------------
+// Stage 1: the incidence record (word + column slots, one load) and the
+// cell's vertex ids.  Stage 2: the relabelled cell's vertex records.
+template <int D, int P>
+struct Stage1 {
+  uint32_t rw[El<D, P>::RS / 4];  // record words: [0] = word, then slot bytes
+  uint32_t v[D + 1];
+};
+
+template <int D, int P>
+struct Stage2 {
+  uint32_t rw[El<D, P>::RS / 4];
+  double x[D + 1][D];
+  double kap[D + 1];
+  double f[D + 1];
+};
+
+template <int D, int P>
+__device__ __forceinline__ Stage1<D, P> fetch1(const AsmParams& p, uint32_t ii) {
+  using E = El<D, P>;
+  Stage1<D, P> s;
+  if constexpr (E::RS == 16) {
+    const uint4 r = __ldg(reinterpret_cast<const uint4*>(p.rec) + ii);
+    s.rw[0] = r.x; s.rw[1] = r.y; s.rw[2] = r.z; s.rw[3] = r.w;
+  } else {
+    const uint2 r = __ldg(reinterpret_cast<const uint2*>(p.rec) + ii);
+    s.rw[0] = r.x; s.rw[1] = r.y;
+  }
+  load_verts<D>(p, s.rw[0] & 0x0fffffffu, s.v);
+  return s;
+}
+
+template <int D, int P, bool FP1>
+__device__ __forceinline__ Stage2<D, P> fetch2(const AsmParams& p, const Stage1<D, P>& s1) {
+  Stage2<D, P> s;
+#pragma unroll
+  for (int q = 0; q < El<D, P>::RS / 4; ++q) s.rw[q] = s1.rw[q];
+  uint32_t pv[D + 1];
+  relabel<D>(s1.v, perm_of<D>(int(s1.rw[0] >> 28)), pv);
+  load_vertex_data<D, FP1>(p, pv, s.x, s.kap, s.f);
+  return s;
+}
+
+template <int D, int P>
+__device__ __forceinline__ uint32_t slot_of(const uint32_t (&rw)[El<D, P>::RS / 4], int j) {
+  const int b = 4 + j;  // byte offset in the record
+  return (rw[b >> 2] >> (8 * (b & 3))) & 0xffu;
+}
+
 // One tile: rows [t.n0, t.n1) of test component t.comp.  `acc` holds the
-// tile's CSR value segment.  Works for any blockDim >= units of the tile.
+// tile's CSR value segment.  Works for any blockDim (threads loop over units).
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
 __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, double* acc) {
   using E = El<D, P>;
   constexpr int BS = FORM == FORM_ELAS ? D : 1;
+  constexpr bool FP1 = LOADM == LOAD_P1;
+  using S1 = Stage1<D, P>;
+  using S2 = Stage2<D, P>;
   const int32_t r0 = __ldg(p.node_rowptr + t.n0), r1 = __ldg(p.node_rowptr + t.n1);
   const int seg = BS * (r1 - r0);
   for (int i = threadIdx.x; i < seg; i += blockDim.x) acc[i] = 0.0;
@@ -340,38 +429,31 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
     double* my = acc + BS * (ra - r0) + e * L;
     const uint32_t i0 = __ldg(p.inc_ptr + node), i1 = __ldg(p.inc_ptr + node + 1);
     double bsum = 0.0;
+    S1 b1{};
+    S2 cur{};
+    if (i0 < i1) {
+      const S1 a1 = fetch1<D, P>(p, i0);
+      if (i0 + 1 < i1) b1 = fetch1<D, P>(p, i0 + 1);
+      cur = fetch2<D, P, FP1>(p, a1);
+    }
     for (uint32_t ii = i0; ii < i1; ++ii) {
-      const uint32_t word = __ldg(p.inc + ii);
-      const uint32_t cell = word & 0x0fffffffu;
-      const int li = int(word >> 28);
+      S2 nxt{};
+      S1 c1{};
+      if (ii + 1 < i1) nxt = fetch2<D, P, FP1>(p, b1);
+      if (ii + 2 < i1) c1 = fetch1<D, P>(p, ii + 2);
+      const int li = int(cur.rw[0] >> 28);
       const bool vertex = li <= D;
-      uint32_t pv[D + 1], code;
-      load_cell<D>(p, cell, li, pv, code);
-      double x[D + 1][D];
-      load_coords<D>(p, pv, x);
-      double kap[D + 1];
-      if constexpr (KP1)
-        for (int a = 0; a <= D; ++a) kap[a] = __ldg(p.kappa + pv[a]);
       Geometry<D> G;
-      geometry(x, G);
+      geometry(cur.x, G);
       CT out[E::K];
-      element_row<D, P, FORM, KP1, CT>(p, G, vertex, t.comp, e, kap, out);
-      const uint32_t* pw = reinterpret_cast<const uint32_t*>(p.pos + size_t(ii) * E::KP);
-      uint32_t w[E::KP / 4];
-      for (int q = 0; q < E::KP / 4; ++q) w[q] = __ldg(pw + q);
+      element_row<D, P, FORM, KP1, CT>(p, G, vertex, t.comp, e, cur.kap, out);
 #pragma unroll
-      for (int j = 0; j < E::K; ++j) {
-        const uint32_t slot = (w[j >> 2] >> (8 * (j & 3))) & 0xffu;
-        my[slot] += double(out[j]);
-      }
+      for (int j = 0; j < E::K; ++j) my[slot_of<D, P>(cur.rw, j)] += double(out[j]);
       if constexpr (LOADM != LOAD_NONE) {
-        if (e == 0) {
-          double fv[D + 1];
-          if constexpr (LOADM == LOAD_P1)
-            for (int a = 0; a <= D; ++a) fv[a] = __ldg(p.f + pv[a]);
-          bsum += load_row<D, P, LOADM>(p, G, vertex, t.comp, fv);
-        }
+        if (e == 0) bsum += load_row<D, P, LOADM>(p, G, vertex, t.comp, cur.f);
       }
+      cur = nxt;
+      b1 = c1;
     }
     if constexpr (LOADM != LOAD_NONE) {
       if (e == 0) {

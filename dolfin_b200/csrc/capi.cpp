@@ -203,13 +203,15 @@ int db2_pattern_csr_host(db2_pattern P, int32_t* rowptr, int32_t* cols) {
 }
 
 int db2_pattern_plan_info(db2_pattern P, int64_t* nnodes, int64_t* nincidences, int* kp,
-                          int64_t* ntiles) {
+                          int64_t* ntiles, int64_t* ngroups, int64_t* ntypes) {
   return guard([&] {
     need(P, "pattern");
     if (nnodes) *nnodes = P->P->V->nnodes;
     if (nincidences) *nincidences = int64_t(P->P->inc.size());
     if (kp) *kp = P->P->kp;
     if (ntiles) *ntiles = int64_t(P->P->tiles.size());
+    if (ngroups) *ngroups = 0;
+    if (ntypes) *ntypes = 0;
   });
 }
 

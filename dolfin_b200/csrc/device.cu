@@ -45,10 +45,11 @@ void DeviceBuffer::upload(const void* host, size_t nbytes) {
   if (e != cudaSuccess) fail(DB2_ERR_CUDA, "cudaMemcpy H2D: %s", cudaGetErrorString(e));
 }
 
-// Coordinates are stored padded (4 doubles per vertex in 3D, 2 in 2D) so that
-// a vertex is one aligned vector load.
+// Vertex records of 4 doubles -- (x, y, z, kappa) in 3D, (x, y, kappa, f) in
+// 2D -- so that a vertex is one aligned 256-bit load; the coefficient slots
+// are written per assembly call (pack_vertex_records).
 void Mesh::upload_coordinates() {
-  const int w = tdim == 3 ? 4 : 2;
+  const int w = 4;
   std::vector<double> pad(size_t(nv) * w, 0.0);
   for (int64_t v = 0; v < nv; ++v)
     for (int r = 0; r < tdim; ++r) pad[v * w + r] = x[v * tdim + r];

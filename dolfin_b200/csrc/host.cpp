@@ -283,6 +283,10 @@ void canonical_node_map(int tdim, int degree, int li, int* map) {
 // incident cells in ascending order -- the order in which DOLFIN's cell loop
 // adds their contributions to row i.
 // ---------------------------------------------------------------------------
+// Tiles: contiguous node ranges with at most one row unit (node x trial
+// block) per thread whose row segment (one test component) fits
+// seg_cap_doubles.
+
 static void build_tiles(Pattern& P, int tile_threads, int seg_cap_doubles) {
   const int bs = P.bs;
   const int64_t nn = P.V->nnodes;
@@ -304,17 +308,42 @@ static void build_tiles(Pattern& P, int tile_threads, int seg_cap_doubles) {
     comp0.push_back(Tile{0, int32_t(n0), int32_t(n1), 0});
     n0 = n1;
   }
+  std::vector<Tile> all;
   for (int c = 0; c < bs; ++c)
     for (auto t : comp0) {
       t.comp = c;
-      P.tiles.push_back(t);
+      all.push_back(t);
     }
   P.seg_cap = max_seg;
+  // Group tiles by the shared memory their row segment needs, so that small
+  // (e.g. edge-node) tiles are not launched with the largest tile's
+  // allocation: one launch per class.
+  static const int kClass[] = {4096, 8192, 12288, 16384, 24576, 32768, 49152, 65536,
+                               98304, 131072, 163840, 196608, 227 * 1024};
+  const int ncls = int(sizeof(kClass) / sizeof(kClass[0]));
+  auto cls_of = [&](const Tile& t) {
+    const int64_t need = int64_t(bs) * (P.node_rowptr[t.n1] - P.node_rowptr[t.n0]) * 8;
+    int k = 0;
+    while (k < ncls - 1 && kClass[k] < need) ++k;
+    return k;
+  };
+  std::stable_sort(all.begin(), all.end(), [&](const Tile& a, const Tile& b) { return cls_of(a) < cls_of(b); });
+  P.tiles = all;
+  P.class_begin.clear();
+  P.class_smem.clear();
+  for (size_t i = 0; i < all.size(); ++i) {
+    const int k = cls_of(all[i]);
+    if (i == 0 || k != cls_of(all[i - 1])) {
+      P.class_begin.push_back(int32_t(i));
+      P.class_smem.push_back(kClass[k]);
+    }
+  }
+  P.class_begin.push_back(int32_t(all.size()));
 }
 
 void retile(Pattern& P, int tile_threads, int seg_cap_bytes) {
   if (tile_threads <= 0 || tile_threads > 1024 || tile_threads % 32)
-    fail(DB2_ERR_ARGUMENT, "tile_threads must be a positive multiple of 32 (<= 1024)");
+    fail(DB2_ERR_ARGUMENT, "tile_threads must be a positive multiple of 32 (<= 256)");
   if (seg_cap_bytes < 1024 || seg_cap_bytes > 220 * 1024)
     fail(DB2_ERR_ARGUMENT, "seg_cap_bytes out of range");
   build_tiles(P, tile_threads, seg_cap_bytes / 8);
@@ -405,7 +434,6 @@ std::shared_ptr<Pattern> make_pattern(std::shared_ptr<Space> V, bool keep_diagon
   if (tile_threads <= 0) tile_threads = 128;
   if (seg_cap_bytes <= 0) seg_cap_bytes = 64 * 1024;
   build_tiles(*P, tile_threads, seg_cap_bytes / 8);
-
   return P;
 }
 
@@ -428,8 +456,15 @@ void Pattern::ensure_device() {
   if (on_device) return;
   d_node_rowptr.upload(node_rowptr.data(), node_rowptr.size() * sizeof(int32_t));
   d_inc_ptr.upload(inc_ptr.data(), inc_ptr.size() * sizeof(uint32_t));
-  d_inc.upload(inc.data(), inc.size() * sizeof(uint32_t));
-  d_pos.upload(pos.data(), pos.size());
+  {
+    rs = 4 + V->k <= 8 ? 8 : 16;
+    std::vector<uint8_t> rec(inc.size() * size_t(rs), 0);
+    for (size_t i = 0; i < inc.size(); ++i) {
+      std::memcpy(&rec[i * rs], &inc[i], 4);
+      std::memcpy(&rec[i * rs + 4], &pos[i * kp], size_t(V->k));
+    }
+    d_rec.upload(rec.data(), rec.size());
+  }
   d_cell_inc.upload(cell_inc.data(), cell_inc.size() * sizeof(uint32_t));
   d_tiles.upload(tiles.data(), tiles.size() * sizeof(Tile));
   launch_expand_csr(*this);

@@ -88,10 +88,16 @@ struct Pattern {
   std::vector<uint8_t> pos;          // inc.size() * kp: column slot (within the node row)
                                      // of each node of the relabelled cell
   std::vector<uint32_t> cell_inc;    // nc * k: incidence index of (cell, local node)
-  std::vector<Tile> tiles;
-  int tile_threads = 128;
-  int seg_cap = 0;                   // doubles of shared memory per tile
-  DeviceBuffer d_node_rowptr, d_inc_ptr, d_inc, d_pos, d_cell_inc, d_tiles, d_rowptr, d_cols;
+  std::vector<Tile> tiles;           // grouped by shared-memory class
+  std::vector<int32_t> class_begin;  // tiles[class_begin[k] .. class_begin[k+1]) share
+  std::vector<int32_t> class_smem;   //   a launch with class_smem[k] bytes of smem
+  int tile_threads = 128;            // CTA size of the tile kernel
+
+  int seg_cap = 0;                   // doubles of shared memory of the largest tile
+  // device incidence records: u32 word then the k slot bytes, padded to
+  // rs = 8 or 16 bytes (one vector load per incidence)
+  int rs = 8;
+  DeviceBuffer d_node_rowptr, d_inc_ptr, d_rec, d_cell_inc, d_tiles, d_rowptr, d_cols;
   bool on_device = false;
   void ensure_device();      // first GPU use: upload the plan, expand the CSR
   // dof-level CSR on the host (component expansion of the node graph)

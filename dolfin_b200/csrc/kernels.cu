@@ -17,25 +17,43 @@ __global__ void __launch_bounds__(256) k_assemble_vector(const AsmParams p, int 
   const int64_t node = r - int64_t(c) * p.nnodes;
   double bsum = 0.0;
   for (uint32_t ii = __ldg(p.inc_ptr + node); ii < __ldg(p.inc_ptr + node + 1); ++ii) {
-    const uint32_t word = __ldg(p.inc + ii);
-    const uint32_t cell = word & 0x0fffffffu;
-    const int li = int(word >> 28);
-    uint32_t pv[D + 1], code;
-    load_cell<D>(p, cell, li, pv, code);
-    double x[D + 1][D];
-    load_coords<D>(p, pv, x);
+    const Stage2<D, P> s = fetch2<D, P, LOADM == LOAD_P1>(p, fetch1<D, P>(p, ii));
     Geometry<D> G;
-    geometry(x, G);
-    double fv[D + 1];
-    if constexpr (LOADM == LOAD_P1)
-      for (int a = 0; a <= D; ++a) fv[a] = __ldg(p.f + pv[a]);
-    bsum += load_row<D, P, LOADM>(p, G, li <= D, c, fv);
+    geometry(s.x, G);
+    bsum += load_row<D, P, LOADM>(p, G, int(s.rw[0] >> 28) <= D, c, s.f);
   }
   double* bp = p.b + r;
   *bp = p.add_values ? *bp + bsum : bsum;
 }
 
+// Vertex records for one call: the w slots of (x, y, z, w) carry kappa (3D);
+// 2D records are (x, y, kappa, f).
+__global__ void k_pack_vertex_records(double* __restrict__ xw, int64_t nv, int tdim,
+                                      const double* __restrict__ kappa,
+                                      const double* __restrict__ f) {
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  if (tdim == 3) {
+    xw[4 * v + 3] = kappa ? kappa[v] : 0.0;
+  } else {
+    xw[4 * v + 2] = kappa ? kappa[v] : 0.0;
+    xw[4 * v + 3] = f ? f[v] : 0.0;
+  }
+}
+
 }  // namespace dev
+
+// Writes kappa (and f in 2D) into the mesh's vertex records on `stream`.
+void pack_vertex_records(const Pattern& P, const double* kappa, const double* f, void* stream) {
+  const Mesh& m = *P.V->mesh;
+  if (!kappa && !(m.tdim == 2 && f)) return;
+  const int threads = 256;
+  dev::k_pack_vertex_records<<<unsigned((m.nv + threads - 1) / threads), threads, 0,
+                               static_cast<cudaStream_t>(stream)>>>(
+      m.d_x.as<double>(), m.nv, m.tdim, kappa, f);
+  count_launch();
+  check_cuda("pack_vertex_records launch");
+}
 
 dev::AsmParams make_params(const Pattern& P) {
   const_cast<Pattern&>(P).ensure_device();
@@ -44,10 +62,9 @@ dev::AsmParams make_params(const Pattern& P) {
   p.tiles = P.d_tiles.as<Tile>();
   p.node_rowptr = P.d_node_rowptr.as<int32_t>();
   p.inc_ptr = P.d_inc_ptr.as<uint32_t>();
-  p.inc = P.d_inc.as<uint32_t>();
-  p.pos = P.d_pos.as<uint8_t>();
+  p.rec = P.d_rec.as<unsigned char>();
   p.cells = m.d_cells.as<uint32_t>();
-  p.x = m.d_x.as<double>();
+  p.xw = m.d_x.as<double>();
   p.cell_nodes = P.V->d_cell_nodes.as<uint32_t>();
   p.cell_inc = P.d_cell_inc.as<uint32_t>();
   p.kscale = 1.0;
@@ -106,6 +123,7 @@ void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int
   p.bc_vals = bc_vals;
   const int loadm = load_mode(L, P.bs, p);
   if (!a) {
+    pack_vertex_records(P, nullptr, loadm == dev::LOAD_P1 ? p.f : nullptr, stream);
     // rank-1 form only
     if (loadm == dev::LOAD_NONE) fail(DB2_ERR_ARGUMENT, "nothing to assemble");
     const int64_t n = V.nnodes * P.bs;
@@ -126,9 +144,9 @@ void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int
   }
   if (bc_flags) fail(DB2_ERR_UNSUPPORTED, "Dirichlet modification not provided by this kernel");
   dev::LaunchCfg cfg;
-  cfg.ntiles = int(P.tiles.size());
+  cfg.class_begin = &P.class_begin;
+  cfg.class_smem = &P.class_smem;
   cfg.threads = P.tile_threads;
-  cfg.smem = size_t(P.seg_cap) * sizeof(double);
   cfg.stream = static_cast<cudaStream_t>(stream);
   const bool fp32 = precision == DB2_FP32_CONTRACT;
   if (precision != DB2_FP64 && precision != DB2_FP32_CONTRACT) fail(DB2_ERR_ARGUMENT, "unknown precision %d", precision);
@@ -136,6 +154,7 @@ void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int
   if (a->f.kind == DB2_FORM_DIFFUSION) {
     if (P.bs != 1) fail(DB2_ERR_UNSUPPORTED, "diffusion form on a vector space");
     const bool kp1 = matrix_coeff(*a, p);
+    pack_vertex_records(P, kp1 ? p.kappa : nullptr, loadm == dev::LOAD_P1 ? p.f : nullptr, stream);
     ok = D == 3 ? dev::dispatch_tet_diff(V.degree, p, cfg, kp1, loadm, fp32)
                 : dev::dispatch_tri_diff(V.degree, p, cfg, kp1, loadm, fp32);
   } else if (a->f.kind == DB2_FORM_ELASTICITY) {
@@ -143,6 +162,7 @@ void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int
     p.mu = a->f.mu;
     p.lmbda = a->f.lmbda;
     if (a->f.coeff != DB2_COEFF_NONE) fail(DB2_ERR_UNSUPPORTED, "elasticity takes no coefficient");
+    pack_vertex_records(P, nullptr, nullptr, stream);
     ok = dev::dispatch_tet_elas(V.degree, p, cfg, false, loadm, fp32);
   } else {
     fail(DB2_ERR_ARGUMENT, "bilinear form kind %d not provided", a->f.kind);

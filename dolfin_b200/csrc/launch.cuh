@@ -1,15 +1,17 @@
 // launch.cuh -- shared launch helpers for the assembly kernel instantiations.
 #pragma once
 
+#include <vector>
+
 #include "assemble.cuh"
 
 namespace db2 {
 namespace dev {
 
 struct LaunchCfg {
-  int ntiles;
+  const std::vector<int32_t>* class_begin;  // tile ranges launched together
+  const std::vector<int32_t>* class_smem;
   int threads;
-  size_t smem;
   cudaStream_t stream;
 };
 
@@ -21,8 +23,16 @@ void run_assemble(const AsmParams& p, const LaunchCfg& cfg) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     configured = true;
   }
-  kern<<<cfg.ntiles, cfg.threads, cfg.smem, cfg.stream>>>(p);
-  count_launch();
+  const auto& cb = *cfg.class_begin;
+  for (size_t k = 0; k + 1 < cb.size(); ++k) {
+    const int n = cb[k + 1] - cb[k];
+    if (n <= 0) continue;
+    AsmParams q = p;
+    q.tiles = p.tiles + cb[k];
+    const size_t smem = size_t((*cfg.class_smem)[k]);
+    kern<<<n, cfg.threads, smem, cfg.stream>>>(q);
+    count_launch();
+  }
   check_cuda("assemble launch");
 }
 

@@ -128,11 +128,12 @@ int db2_pattern_destroy(db2_pattern P);
    incidences in cell order, per-incidence column slots (kp bytes each), and
    tiles as int32 quadruples (component, first node, end node, 0). */
 int db2_pattern_plan_info(db2_pattern P, int64_t* nnodes, int64_t* nincidences, int* kp,
-                          int64_t* ntiles);
+                          int64_t* ntiles, int64_t* ngroups, int64_t* ntypes);
 int db2_pattern_plan_copy(db2_pattern P, int32_t* node_rowptr, int32_t* node_cols,
                           uint32_t* inc_ptr, uint32_t* inc, uint8_t* pos, int32_t* tiles);
-/* Re-cut the pattern's tiles: at most tile_threads row units per CTA and
-   seg_cap_bytes of shared-memory row segment. */
+/* Re-cut the pattern's tiles (launch shape of the assembly kernel): CTAs of
+   tile_threads threads, row segments of at most seg_cap_bytes of shared
+   memory.  Results do not depend on the launch shape (bitwise). */
 int db2_pattern_retile(db2_pattern P, int tile_threads, int seg_cap_bytes);
 
 /* ---- assembly --------------------------------------------------------- */
