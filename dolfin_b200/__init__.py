@@ -15,6 +15,7 @@ hand-written CUDA kernels reached through the C ABI in include/dolfin_b200.h.
 """
 from . import _capi
 from .assembling import SystemAssembler, assemble, assemble_action, assemble_system
+from .bcs import DirichletBC
 from .cpp import (DofMap, FunctionSpace, Mesh, SparsityPattern, UnitCubeMesh, UnitSquareMesh,
                   VectorFunctionSpace, parameters)
 from .function import Constant, Function
@@ -27,6 +28,7 @@ __all__ = [
     "UnitSquareMesh", "FunctionSpace", "VectorFunctionSpace", "DofMap", "SparsityPattern",
     "parameters", "Function", "Constant", "Matrix", "Vector", "TestFunction", "TrialFunction",
     "grad", "inner", "dot", "dx", "div", "sym", "tr", "transpose", "nabla_grad", "Identity",
+    "DirichletBC",
 ]
 
 

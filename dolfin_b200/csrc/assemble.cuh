@@ -209,6 +209,7 @@ DB2_ROWS_EDGE(2, p2tri, 6)
 struct AsmParams {
   const Tile* tiles;
   const int32_t* node_rowptr;
+  const int32_t* cols;       // dof-level CSR column indices (Dirichlet epilogue)
   const uint32_t* inc_ptr;
   const unsigned char* rec;  // incidence records (El::RS bytes each)
   const uint32_t* cells;
@@ -408,7 +409,14 @@ __device__ __forceinline__ uint32_t slot_of(const uint32_t (&rw)[El<D, P>::RS / 
 }
 
 // One tile: rows [t.n0, t.n1) of test component t.comp.  `acc` holds the
-// tile's CSR value segment.  Works for any blockDim (threads loop over units).
+// tile's CSR value segment followed by one double per row unit (load-vector
+// partials).  blockDim must be at least the tile's unit count.
+//
+// With Dirichlet data (p.bc_flags) each element row is modified as
+// SystemAssembler::apply_bc (dolfin/fem/SystemAssembler.cpp:1037-1070) does
+// per cell: a Dirichlet row keeps only 1 on its diagonal and contributes g_i
+// to b; other rows move their Dirichlet-column entries to b (b_i -= A_ij g_j)
+// and zero them.
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
 __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, double* acc) {
   using E = El<D, P>;
@@ -418,10 +426,13 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
   using S2 = Stage2<D, P>;
   const int32_t r0 = __ldg(p.node_rowptr + t.n0), r1 = __ldg(p.node_rowptr + t.n1);
   const int seg = BS * (r1 - r0);
+  double* bpart = acc + seg;
   for (int i = threadIdx.x; i < seg; i += blockDim.x) acc[i] = 0.0;
   __syncthreads();
   const int units = (t.n1 - t.n0) * BS;
-  for (int u = threadIdx.x; u < units; u += blockDim.x) {
+  const bool bc = p.bc_flags != nullptr;
+  if (int(threadIdx.x) < units) {
+    const int u = threadIdx.x;
     const int node = t.n0 + u / BS;
     const int e = u % BS;
     const int32_t ra = __ldg(p.node_rowptr + node);
@@ -429,6 +440,15 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
     double* my = acc + BS * (ra - r0) + e * L;
     const uint32_t i0 = __ldg(p.inc_ptr + node), i1 = __ldg(p.inc_ptr + node + 1);
     double bsum = 0.0;
+    const int64_t rowdof = int64_t(t.comp) * p.nnodes + node;
+    bool row_bc = false;
+    double row_g = 0.0;
+    const int32_t* colrow = nullptr;
+    if (bc) {
+      row_bc = __ldg(p.bc_flags + rowdof) != 0;
+      row_g = row_bc ? __ldg(p.bc_vals + rowdof) : 0.0;
+      colrow = p.cols + int64_t(t.comp) * BS * p.nnz_node + int64_t(BS) * ra + e * L;
+    }
     S1 b1{};
     S2 cur{};
     if (i0 < i1) {
@@ -447,22 +467,47 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
       geometry(cur.x, G);
       CT out[E::K];
       element_row<D, P, FORM, KP1, CT>(p, G, vertex, t.comp, e, cur.kap, out);
-#pragma unroll
-      for (int j = 0; j < E::K; ++j) my[slot_of<D, P>(cur.rw, j)] += double(out[j]);
       if constexpr (LOADM != LOAD_NONE) {
         if (e == 0) bsum += load_row<D, P, LOADM>(p, G, vertex, t.comp, cur.f);
       }
+      if (bc) {
+        if (row_bc) {
+          // the row node is relabelled local node 0 (vertex) or K-1 (edge (0,1))
+          const int jstar = vertex ? 0 : E::K - 1;
+#pragma unroll
+          for (int j = 0; j < E::K; ++j) out[j] = CT((e == t.comp && j == jstar) ? 1 : 0);
+          if constexpr (LOADM != LOAD_NONE) {
+            if (e == 0) bsum = bsum - load_row<D, P, LOADM>(p, G, vertex, t.comp, cur.f) + row_g;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < E::K; ++j) {
+            const int32_t dof = __ldg(colrow + slot_of<D, P>(cur.rw, j));
+            if (__ldg(p.bc_flags + dof)) {
+              bsum -= double(out[j]) * __ldg(p.bc_vals + dof);
+              out[j] = CT(0);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < E::K; ++j) my[slot_of<D, P>(cur.rw, j)] += double(out[j]);
       cur = nxt;
       b1 = c1;
     }
-    if constexpr (LOADM != LOAD_NONE) {
-      if (e == 0) {
-        double* bp = p.b + int64_t(t.comp) * p.nnodes + node;
-        *bp = p.add_values ? *bp + bsum : bsum;
-      }
-    }
+    bpart[u] = bsum;
   }
   __syncthreads();
+  if constexpr (LOADM != LOAD_NONE) {
+    // b of each row: its trial blocks' partials in block order
+    for (int i = threadIdx.x; i < t.n1 - t.n0; i += blockDim.x) {
+      double s = 0.0;
+#pragma unroll
+      for (int e = 0; e < BS; ++e) s += bpart[i * BS + e];
+      double* bp = p.b + int64_t(t.comp) * p.nnodes + t.n0 + i;
+      *bp = p.add_values ? *bp + s : s;
+    }
+  }
   double* dst = p.vals + int64_t(t.comp) * BS * p.nnz_node + int64_t(BS) * r0;
   if (p.add_values) {
     for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] += acc[i];

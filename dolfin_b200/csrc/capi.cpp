@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <new>
 #include <string>
@@ -22,6 +23,7 @@ struct db2_pattern_t {
 
 namespace db2 {
 int64_t launches();
+std::shared_ptr<Pattern> pattern_of(db2_pattern P) { return P ? P->P : nullptr; }
 }
 
 namespace {
@@ -58,6 +60,10 @@ db2::FormArgs form_args(const db2_form* f, const double* w) {
   return a;
 }
 }  // namespace
+
+namespace db2 {
+int guard_call(const std::function<void()>& f) { return guard(f); }
+}
 
 extern "C" {
 

@@ -287,11 +287,9 @@ void canonical_node_map(int tdim, int degree, int li, int* map) {
 // block) per thread whose row segment (one test component) fits
 // seg_cap_doubles.
 
-static void build_tiles(Pattern& P, int tile_threads, int seg_cap_doubles) {
+std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doubles, int* max_seg_out) {
   const int bs = P.bs;
   const int64_t nn = P.V->nnodes;
-  P.tiles.clear();
-  P.tile_threads = tile_threads;
   int max_seg = 0;
   std::vector<Tile> comp0;
   int64_t n0 = 0;
@@ -314,6 +312,15 @@ static void build_tiles(Pattern& P, int tile_threads, int seg_cap_doubles) {
       t.comp = c;
       all.push_back(t);
     }
+  if (max_seg_out) *max_seg_out = max_seg;
+  return all;
+}
+
+static void build_tiles(Pattern& P, int tile_threads, int seg_cap_doubles) {
+  const int bs = P.bs;
+  P.tile_threads = tile_threads;
+  int max_seg = 0;
+  std::vector<Tile> all = cut_tiles(P, tile_threads, seg_cap_doubles, &max_seg);
   P.seg_cap = max_seg;
   // Group tiles by the shared memory their row segment needs, so that small
   // (e.g. edge-node) tiles are not launched with the largest tile's
@@ -342,7 +349,7 @@ static void build_tiles(Pattern& P, int tile_threads, int seg_cap_doubles) {
 }
 
 void retile(Pattern& P, int tile_threads, int seg_cap_bytes) {
-  if (tile_threads <= 0 || tile_threads > 1024 || tile_threads % 32)
+  if (tile_threads <= 0 || tile_threads > 256 || tile_threads % 32)
     fail(DB2_ERR_ARGUMENT, "tile_threads must be a positive multiple of 32 (<= 256)");
   if (seg_cap_bytes < 1024 || seg_cap_bytes > 220 * 1024)
     fail(DB2_ERR_ARGUMENT, "seg_cap_bytes out of range");

@@ -120,6 +120,8 @@ std::shared_ptr<Pattern> make_pattern(std::shared_ptr<Space> V, bool keep_diagon
                                       int tile_threads = 0, int seg_cap_bytes = 0);
 // Re-cut the tiles of an existing plan (autotuning), re-uploading d_tiles.
 void retile(Pattern& P, int tile_threads, int seg_cap_bytes);
+// Tiles of a pattern for a launch shape (pure; does not modify P).
+std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doubles, int* max_seg);
 
 // Launchers (kernels.cu).  All return after enqueueing on `stream`.
 struct FormArgs {

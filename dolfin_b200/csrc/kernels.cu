@@ -142,7 +142,8 @@ void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int
 #undef DB2_VEC
     fail(DB2_ERR_UNSUPPORTED, "vector assembly not provided for this element");
   }
-  if (bc_flags) fail(DB2_ERR_UNSUPPORTED, "Dirichlet modification not provided by this kernel");
+  if (bc_flags && (!bc_vals || !L || !b)) fail(DB2_ERR_ARGUMENT, "Dirichlet data needs values, a linear form and b");
+  p.cols = P.d_cols.as<int32_t>();
   dev::LaunchCfg cfg;
   cfg.class_begin = &P.class_begin;
   cfg.class_smem = &P.class_smem;

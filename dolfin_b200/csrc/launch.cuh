@@ -29,7 +29,7 @@ void run_assemble(const AsmParams& p, const LaunchCfg& cfg) {
     if (n <= 0) continue;
     AsmParams q = p;
     q.tiles = p.tiles + cb[k];
-    const size_t smem = size_t((*cfg.class_smem)[k]);
+    const size_t smem = size_t((*cfg.class_smem)[k]) + size_t(cfg.threads) * sizeof(double);
     kern<<<n, cfg.threads, smem, cfg.stream>>>(q);
     count_launch();
   }
