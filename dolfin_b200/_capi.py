@@ -70,6 +70,7 @@ _SIGS = {
     "db2_assemble_system_bc": [P, P, P, P, P, P, P, I, P, P, P],
     "db2_apply": [P, P, P, I, P, P, P],
     "db2_vjp_kappa": [P, P, P, P, P, P, P, I, P, P],
+    "db2_vjp_kappa_noalloc": [P, P, P, P, P, P, P, I, P, P],
     "db2_batch_create": [I, P, P, P, P, I, I, I, PP],
     "db2_batch_info": [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I)],
     "db2_batch_assemble": [P, I, P],

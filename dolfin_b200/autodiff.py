@@ -22,8 +22,11 @@ def _p(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
 
 
-def vjp_kappa(V, kappa, gA, f=None, gb=None, precision="fp64", scale=1.0):
-    """dL/dkappa (vertex field) for a = scale*kappa*grad(u).grad(v)*dx on V."""
+def vjp_kappa(V, kappa, gA, f=None, gb=None, precision="fp64", scale=1.0, noalloc=False):
+    """dL/dkappa (vertex field) for a = scale*kappa*grad(u).grad(v)*dx on V.
+
+    noalloc=True uses db2_vjp_kappa_noalloc: the engine allocates no device
+    memory during the call (fixed work array; see include/dolfin_b200.h)."""
     P = V.pattern()
     nv = V.mesh().num_vertices()
     kappa = kappa.contiguous().to(torch.float64)
@@ -37,7 +40,7 @@ def vjp_kappa(V, kappa, gA, f=None, gb=None, precision="fp64", scale=1.0):
         f = f.contiguous().to(torch.float64)
         gb = gb.contiguous().to(torch.float64)
     dk = torch.empty(nv, dtype=torch.float64, device=kappa.device)
-    call("db2_vjp_kappa", P.handle, C.byref(a), _p(kappa), C.byref(L) if L is not None else None,
+    call("db2_vjp_kappa_noalloc" if noalloc else "db2_vjp_kappa", P.handle, C.byref(a), _p(kappa), C.byref(L) if L is not None else None,
          _p(f), _p(gA), _p(gb), _PREC[precision], _p(dk), _stream())
     return dk
 

@@ -172,6 +172,24 @@ int db2_vjp_kappa(db2_pattern P, const db2_form* a, const double* kappa, const d
                   const double* f, const double* gA, const double* gb, int precision,
                   double* dkappa, void* stream);
 
+/* Allocation-free variant of db2_vjp_kappa (no counterpart in the
+   reference).  For callers that cannot let a library allocate device memory
+   at call time -- applications whose device memory belongs to their own pool
+   allocator, or loops with streams in flight that cudaMalloc's implicit
+   synchronisation would stall.  Same arguments and result as
+   db2_vjp_kappa, but the work array is a fixed array inside the library:
+   at most 2^21 doubles, i.e. cells * (tdim + 1) <= 2097152 (524,288
+   tetrahedra / 699,050 triangles); larger patterns fail with DB2_ERR_SHAPE.
+   It calls no cudaMalloc/cudaFree: the pattern must already be resident on
+   the device (after any assembly with it, or db2_pattern_csr_device).  The
+   first call on each device looks up the array's device address
+   (cudaGetSymbolAddress) and should come before any stream capture.  All
+   calls share the one array, so calls that overlap on the GPU (other
+   streams, other threads) race; order them on one stream. */
+int db2_vjp_kappa_noalloc(db2_pattern P, const db2_form* a, const double* kappa,
+                          const db2_form* L, const double* f, const double* gA,
+                          const double* gb, int precision, double* dkappa, void* stream);
+
 /* ---- batched multi-mesh assembly -------------------------------------- */
 /* A batch of patterns (any element/space mix) assembled by ONE persistent
    launch.  kappa pointers (device, one P1 field per member) and output
