@@ -10,7 +10,7 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libdolfin_b200.so")
+LIB_PATH = os.environ.get("DOLFIN_B200_LIB") or os.path.join(_HERE, "_lib", "libdolfin_b200.so")
 
 DB2_OK = 0
 ERR_NAMES = {1: "argument", 2: "shape", 3: "index", 4: "mesh", 5: "unsupported", 6: "cuda",

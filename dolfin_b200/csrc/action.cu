@@ -7,42 +7,9 @@
 namespace db2 {
 namespace dev {
 
-// Local edge index of the unordered local vertex pair (p, q), p != q.
-template <int D>
-__device__ __forceinline__ int edge_of(int p, int q) {
-  const int lo = p < q ? p : q, hi = p < q ? q : p;
-  if constexpr (D == 3) {
-    // (2,3)->0 (1,3)->1 (1,2)->2 (0,3)->3 (0,2)->4 (0,1)->5
-    if (lo == 0) return hi == 1 ? 5 : (hi == 2 ? 4 : 3);
-    if (lo == 1) return hi == 2 ? 2 : 1;
-    return 0;
-  } else {
-    // (1,2)->0 (0,2)->1 (0,1)->2
-    if (lo == 0) return hi == 1 ? 2 : 1;
-    return 0;
-  }
-}
-
-// Global nodes of the relabelled cell in its local order (vertices = vertex
-// ids; P2 edge nodes through the cell's node list).
-template <int D, int P>
-__device__ __forceinline__ void relabelled_nodes(const AsmParams& p, uint32_t cell, uint32_t code,
-                                                 const uint32_t (&pv)[D + 1],
-                                                 uint32_t (&nodes)[El<D, P>::K]) {
-  using E = El<D, P>;
-  for (int a = 0; a <= D; ++a) nodes[a] = pv[a];
-  if constexpr (P == 2) {
-    const uint32_t* cn = p.cell_nodes + size_t(cell) * E::K;
-    for (int e2 = 0; e2 < E::NE; ++e2) {
-      const int A = edge_end(D, e2, 0), B = edge_end(D, e2, 1);
-      const int pa = int((code >> (2 * A)) & 3u), pb = int((code >> (2 * B)) & 3u);
-      nodes[E::NV + e2] = __ldg(cn + E::NV + edge_of<D>(pa, pb));
-    }
-  }
-}
-
 // y[(c,i)] = sum over cells K around node i of sum_{e,j} A^K_{(c,i),(e,j)} x[(e,j)]
-// (one thread per dof row, register accumulation in cell order).
+// (one thread per dof row, register accumulation in cell order; the x index
+// of column slot q of block e is the CSR column itself).
 template <int D, int P, int FORM, bool KP1, typename CT>
 __global__ void __launch_bounds__(256) k_apply(const AsmParams p, const double* __restrict__ xin,
                                                double* __restrict__ y) {
@@ -51,29 +18,27 @@ __global__ void __launch_bounds__(256) k_apply(const AsmParams p, const double* 
   const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= p.nnodes * BS) return;
   const int c = int(r / p.nnodes);
-  const int64_t node = r - int64_t(c) * p.nnodes;
+  const uint32_t node = uint32_t(r - int64_t(c) * p.nnodes);
+  const int32_t ra = __ldg(p.node_rowptr + node);
+  const int32_t L = __ldg(p.node_rowptr + node + 1) - ra;
+  const int32_t* crow = p.cols + int64_t(c) * BS * p.nnz_node + int64_t(BS) * ra;
+  const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - __ldg(p.inc_ptr + node);
+  const uint32_t rbase = __ldg(p.rec_goff + (node >> 5)) + (node & 31u);
+  const RowFix<D> F = load_row_fix<D, P, false>(p, node);
   double acc = 0.0;
-  for (uint32_t ii = __ldg(p.inc_ptr + node); ii < __ldg(p.inc_ptr + node + 1); ++ii) {
-    const uint32_t word = rec_word<D, P>(p, ii);
-    const uint32_t cell = word & 0x0fffffffu;
-    const int li = int(word >> 28);
-    const uint32_t code = perm_of<D>(li);
-    uint32_t v[D + 1], pv[D + 1];
-    load_verts<D>(p, cell, v);
-    relabel<D>(v, code, pv);
+  for (uint32_t m = 0; m < cnt; ++m) {
+    const Rec<D, P> rr = load_rec<D, P>(p, rbase + 32u * m);
     double x[D + 1][D], kap[D + 1], fv[D + 1];
-    load_vertex_data<D, false>(p, pv, x, kap, fv);
+    record_cell<D, P, false>(p, F, rr, x, kap, fv);
     Geometry<D> G;
     geometry(x, G);
-    uint32_t nodes[E::K];
-    relabelled_nodes<D, P>(p, cell, code, pv, nodes);
 #pragma unroll 1
     for (int e = 0; e < BS; ++e) {
       CT out[E::K];
-      element_row<D, P, FORM, KP1, CT>(p, G, li <= D, c, e, kap, out);
-      const double* xe = xin + int64_t(e) * p.nnodes;
+      element_row<D, P, FORM, KP1, CT>(p, G, F.nfix == 1, c, e, kap, out);
 #pragma unroll
-      for (int j = 0; j < E::K; ++j) acc = fma(double(out[j]), __ldg(xe + nodes[j]), acc);
+      for (int j = 0; j < E::K; ++j)
+        acc = fma(double(out[j]), __ldg(xin + __ldg(crow + e * L + rr.slot(j))), acc);
     }
   }
   y[r] = acc;
@@ -110,8 +75,9 @@ __global__ void __launch_bounds__(256) k_vjp_cells(const AsmParams p, int64_t nc
     const bool vertex = li <= D;
     // gA at the row's slots, in the relabelled local order
     double g[E::K];
+    const Rec<D, P> rr = load_rec<D, P>(p, rec_index<D, P>(p, node, ii - __ldg(p.inc_ptr + node)));
 #pragma unroll
-    for (int j = 0; j < E::K; ++j) g[j] = __ldg(grow + rec_slot<D, P>(p, ii, j));
+    for (int j = 0; j < E::K; ++j) g[j] = __ldg(grow + rr.slot(j));
     CT W0[1][NB];
     CT W1[2][NB];
     for (int b = 0; b < NB; ++b) W0[0][b] = CT(ndot<D>(G, 0, b) * (G.s * p.kscale));
@@ -161,7 +127,7 @@ __global__ void __launch_bounds__(256) k_vjp_vertices(const AsmParams p, int64_t
   if (v >= nv) return;
   double s = 0.0;
   for (uint32_t ii = __ldg(p.inc_ptr + v); ii < __ldg(p.inc_ptr + v + 1); ++ii) {
-    const uint32_t word = rec_word<D, P>(p, ii);
+    const uint32_t word = __ldg(p.inc + ii);
     s += __ldg(t + size_t(word & 0x0fffffffu) * (D + 1) + (word >> 28));
   }
   dk[v] = s;

@@ -66,17 +66,6 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_batch(const BatchMember* __
   }
 }
 
-// One launch, one tile per CTA, for member tiles [t0, t0 + n) (reference loop).
-template <typename CT>
-__global__ void __launch_bounds__(kMaxTileThreads) k_batch_member(const BatchMember* __restrict__ members,
-                                                                  const BatchTile* __restrict__ tiles,
-                                                                  int t0) {
-  extern __shared__ double acc[];
-  const BatchTile bt = tiles[t0 + blockIdx.x];
-  const Tile tile{bt.comp, bt.n0, bt.n1, 0};
-  batch_tile<CT>(members[bt.member], tile, acc);
-}
-
 // kappa into the w (3D) or third (2D) slot of every member's vertex records.
 __global__ void k_batch_pack(const BatchMember* __restrict__ members, int nmembers,
                              const int64_t* __restrict__ vstart, int64_t nvtot) {
@@ -115,12 +104,8 @@ struct Batch {
 
 template <typename CT>
 void set_smem_attr() {
-  static bool done = false;
-  if (!done) {
-    cudaFuncSetAttribute(dev::k_batch<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(dev::k_batch_member<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    done = true;
-  }
+  static unsigned long long done = 0;
+  dev::allow_dynamic_smem(dev::k_batch<CT>, done);
 }
 
 void enqueue_pack(Batch& B, cudaStream_t s) {
@@ -140,16 +125,24 @@ void enqueue_persistent(Batch& B, cudaStream_t s) {
   count_launch();
 }
 
+// The reference loop: one launch per member over that member's tiles.  It
+// runs the same k_batch kernel as the persistent path (with the member's tile
+// range and a counter of its own): two kernels that each inline tile_body may
+// be compiled with different multiply-add fusion, and the loop is the check
+// that the persistent schedule does not change a single bit.
 template <typename CT>
 void enqueue_loop(Batch& B, cudaStream_t s) {
-  // per member: its vertex-record pack (a slice of the batched pack is not
-  // separable, so the loop packs all members once) and its own launch
+  // the vertex-record pack covers all members at once (a slice of it is not
+  // separable), then one launch per member
+  const size_t nm = B.members.size();
+  cudaMemsetAsync(B.d_counter.ptr, 0, (nm + 1) * sizeof(unsigned int), s);
   enqueue_pack(B, s);
-  for (size_t m = 0; m < B.members.size(); ++m) {
+  for (size_t m = 0; m < nm; ++m) {
     const int t0 = B.member_first[m], n = B.member_first[m + 1] - t0;
     if (n <= 0) continue;
-    dev::k_batch_member<CT><<<n, B.threads, size_t(B.smem), s>>>(
-        B.d_members.as<dev::BatchMember>(), B.d_member_tiles.as<dev::BatchTile>(), t0);
+    dev::k_batch<CT><<<std::min(n, B.ctas), B.threads, size_t(B.smem), s>>>(
+        B.d_members.as<dev::BatchMember>(), B.d_member_tiles.as<dev::BatchTile>() + t0, n,
+        B.d_counter.as<unsigned int>() + 1 + m);
     count_launch();
   }
 }
@@ -236,7 +229,7 @@ int db2_batch_create(int count, const db2_pattern* patterns, const db2_form* for
       B.d_tiles.upload(B.tiles.data(), B.tiles.size() * sizeof(dev::BatchTile));
       B.d_member_tiles.upload(B.member_tiles.data(), B.member_tiles.size() * sizeof(dev::BatchTile));
       B.d_vstart.upload(B.vstart.data(), B.vstart.size() * sizeof(int64_t));
-      B.d_counter.alloc(sizeof(unsigned int));
+      B.d_counter.alloc((B.members.size() + 1) * sizeof(unsigned int));
       check_cuda("batch create");
     } catch (...) {
       delete h;

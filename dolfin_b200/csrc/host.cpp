@@ -195,13 +195,19 @@ void Mesh::compute_edges() {
   for (int64_t v = 0; v < nv; ++v) nuniq[v + 1] += nuniq[v];
   ne = nuniq[nv];
   cell_edges.assign(nslots, 0);
+  edge_vertices.assign(size_t(ne) * 2, 0);
   parallel_for(nv, [&](int64_t b, int64_t e) {
     for (int64_t v = b; v < e; ++v) {
       int64_t id = int64_t(nuniq[v]) - 1;
       uint64_t prev = ~uint64_t(0);
       for (uint32_t s = start[v]; s < start[v + 1]; ++s) {
         const uint64_t q = bucket[s] >> 32;
-        if (q != prev) { ++id; prev = q; }
+        if (q != prev) {
+          ++id;
+          prev = q;
+          edge_vertices[2 * id] = uint32_t(v);
+          edge_vertices[2 * id + 1] = uint32_t(q);
+        }
         cell_edges[bucket[s] & 0xffffffffu] = uint32_t(id);
       }
     }
@@ -455,6 +461,8 @@ void Space::ensure_device() {
   mesh->ensure_device();
   if (on_device) return;
   d_cell_nodes.upload(cell_nodes.data(), cell_nodes.size() * sizeof(uint32_t));
+  if (degree == 2)
+    d_edge_vertices.upload(mesh->edge_vertices.data(), mesh->edge_vertices.size() * sizeof(uint32_t));
   on_device = true;
 }
 
@@ -463,14 +471,46 @@ void Pattern::ensure_device() {
   if (on_device) return;
   d_node_rowptr.upload(node_rowptr.data(), node_rowptr.size() * sizeof(int32_t));
   d_inc_ptr.upload(inc_ptr.data(), inc_ptr.size() * sizeof(uint32_t));
+  d_inc.upload(inc.data(), inc.size() * sizeof(uint32_t));
   {
-    rs = 4 + V->k <= 8 ? 8 : 16;
-    std::vector<uint8_t> rec(inc.size() * size_t(rs), 0);
-    for (size_t i = 0; i < inc.size(); ++i) {
-      std::memcpy(&rec[i * rs], &inc[i], 4);
-      std::memcpy(&rec[i * rs + 4], &pos[i * kp], size_t(V->k));
+    const Mesh& m = *V->mesh;
+    const int D = m.tdim, K = V->k, nd = D;
+    rs = 2 * nd + K <= 8 ? 8 : 16;
+    const int64_t nn = V->nnodes, ngrp = (nn + 31) / 32;
+    rec_goff.assign(ngrp + 1, 0);
+    for (int64_t g = 0; g < ngrp; ++g) {
+      uint32_t mx = 0;
+      for (int64_t i = 32 * g; i < std::min(nn, 32 * g + 32); ++i) mx = std::max(mx, inc_ptr[i + 1] - inc_ptr[i]);
+      if (uint64_t(rec_goff[g]) + 32ull * mx >= (1ull << 32)) fail(DB2_ERR_UNSUPPORTED, "too many incidence records");
+      rec_goff[g + 1] = rec_goff[g] + 32 * mx;
     }
+    std::vector<uint8_t> rec(size_t(rec_goff[ngrp]) * rs, 0);
+    std::atomic<int64_t> bad{-1};
+    parallel_for(nn, [&](int64_t b, int64_t e) {
+      for (int64_t i = b; i < e; ++i) {
+        for (uint32_t s = inc_ptr[i]; s < inc_ptr[i + 1]; ++s) {
+          const uint32_t c = inc[s] & 0x0fffffffu, li = inc[s] >> 28;
+          int perm[4];
+          canonical_perm(D, int(li), perm);
+          const uint32_t* cv = &m.cells[size_t(c) * (D + 1)];
+          const int nfix = int(li) <= D ? 1 : 2;
+          const int64_t base = cv[perm[0]];
+          uint8_t* r = &rec[(size_t(rec_goff[i >> 5]) + (i & 31) + 32ull * (s - inc_ptr[i])) * rs];
+          for (int a = nfix; a <= D; ++a) {
+            const int64_t d = int64_t(cv[perm[a]]) - base;
+            if (d < -32768 || d > 32767) bad = i;
+            const int16_t d16 = int16_t(d);
+            std::memcpy(r + 2 * (a - nfix), &d16, 2);
+          }
+          std::memcpy(r + 2 * nd, &pos[size_t(s) * kp], size_t(K));
+        }
+      }
+    });
+    if (bad >= 0)
+      fail(DB2_ERR_UNSUPPORTED, "vertex numbering too spread for 16-bit cell offsets (node %lld); "
+           "renumber the mesh vertices for locality", (long long)bad.load());
     d_rec.upload(rec.data(), rec.size());
+    d_rec_goff.upload(rec_goff.data(), rec_goff.size() * sizeof(uint32_t));
   }
   d_cell_inc.upload(cell_inc.data(), cell_inc.size() * sizeof(uint32_t));
   d_tiles.upload(tiles.data(), tiles.size() * sizeof(Tile));

@@ -40,6 +40,7 @@ struct Mesh {
   bool have_edges = false;
   int64_t ne = 0;
   std::vector<uint32_t> cell_edges;  // nc * nedges(tdim), UFC local edge order
+  std::vector<uint32_t> edge_vertices;  // ne * 2, sorted vertex pair of each edge
   // device copies: coordinates padded to 4 (3D) or 2 (2D) doubles per vertex
   DeviceBuffer d_x, d_cells;
   bool on_device = false;
@@ -59,6 +60,7 @@ struct Space {
   int64_t nnodes = 0;     // scalar global dimension
   std::vector<uint32_t> cell_nodes;  // nc * k
   DeviceBuffer d_cell_nodes;
+  DeviceBuffer d_edge_vertices;      // P2: sorted endpoints of each edge node
   bool on_device = false;
   void ensure_device();
   int64_t dim() const { return nnodes * vsize; }
@@ -94,10 +96,14 @@ struct Pattern {
   int tile_threads = 128;            // CTA size of the tile kernel
 
   int seg_cap = 0;                   // doubles of shared memory of the largest tile
-  // device incidence records: u32 word then the k slot bytes, padded to
-  // rs = 8 or 16 bytes (one vector load per incidence)
+  // Device incidence records (rs = 8 or 16 bytes, one vector load each):
+  // int16 offsets, relative to the row's first fixed vertex, of the other
+  // vertices of the relabelled cell, then its k column slots.  Records of
+  // each block of 32 consecutive nodes are interleaved (record m of node i at
+  // rec_goff[i/32] + i%32 + 32 m) so that a warp's loads are contiguous.
   int rs = 8;
-  DeviceBuffer d_node_rowptr, d_inc_ptr, d_rec, d_cell_inc, d_tiles, d_rowptr, d_cols;
+  std::vector<uint32_t> rec_goff;    // per 32-node block: first record index
+  DeviceBuffer d_node_rowptr, d_inc_ptr, d_inc, d_rec, d_rec_goff, d_cell_inc, d_tiles, d_rowptr, d_cols;
   bool on_device = false;
   void ensure_device();      // first GPU use: upload the plan, expand the CSR
   // dof-level CSR on the host (component expansion of the node graph)

@@ -16,11 +16,16 @@ __global__ void __launch_bounds__(256) k_assemble_vector(const AsmParams p, int 
   const int c = int(r / p.nnodes);
   const int64_t node = r - int64_t(c) * p.nnodes;
   double bsum = 0.0;
-  for (uint32_t ii = __ldg(p.inc_ptr + node); ii < __ldg(p.inc_ptr + node + 1); ++ii) {
-    const Stage2<D, P> s = fetch2<D, P, LOADM == LOAD_P1>(p, fetch1<D, P>(p, ii));
+  const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - __ldg(p.inc_ptr + node);
+  const uint32_t rbase = __ldg(p.rec_goff + (node >> 5)) + uint32_t(node & 31);
+  const RowFix<D> F = load_row_fix<D, P, LOADM == LOAD_P1>(p, uint32_t(node));
+  for (uint32_t m = 0; m < cnt; ++m) {
+    const Rec<D, P> r = load_rec<D, P>(p, rbase + 32u * m);
+    double x[D + 1][D], kap[D + 1], fv[D + 1];
+    record_cell<D, P, LOADM == LOAD_P1>(p, F, r, x, kap, fv);
     Geometry<D> G;
-    geometry(s.x, G);
-    bsum += load_row<D, P, LOADM>(p, G, int(s.rw[0] >> 28) <= D, c, s.f);
+    geometry(x, G);
+    bsum += load_row<D, P, LOADM>(p, G, F.nfix == 1, c, fv);
   }
   double* bp = p.b + r;
   *bp = p.add_values ? *bp + bsum : bsum;
@@ -63,6 +68,11 @@ dev::AsmParams make_params(const Pattern& P) {
   p.node_rowptr = P.d_node_rowptr.as<int32_t>();
   p.inc_ptr = P.d_inc_ptr.as<uint32_t>();
   p.rec = P.d_rec.as<unsigned char>();
+  p.rec_goff = P.d_rec_goff.as<uint32_t>();
+  p.inc = P.d_inc.as<uint32_t>();
+  p.cols = P.d_cols.as<int32_t>();
+  p.edge_v = P.V->d_edge_vertices.as<uint32_t>();
+  p.nverts = m.nv;
   p.cells = m.d_cells.as<uint32_t>();
   p.xw = m.d_x.as<double>();
   p.cell_nodes = P.V->d_cell_nodes.as<uint32_t>();

@@ -15,14 +15,30 @@ struct LaunchCfg {
   cudaStream_t stream;
 };
 
+// Let `kern` use all the dynamic shared memory the current device allows a
+// block, less the kernel's own static shared memory (the opt-in limit covers
+// both).  Done once per kernel and device; `done` is the caller's per-kernel
+// record of the devices already configured.
+template <typename Kernel>
+void allow_dynamic_smem(Kernel kern, unsigned long long& done) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && (done >> dev & 1ull)) return;
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa{};
+  cudaFuncGetAttributes(&fa, kern);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       optin - int(fa.sharedSizeBytes));
+  check_cuda("shared-memory allowance");
+  if (dev < 64) done |= 1ull << dev;
+}
+
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
 void run_assemble(const AsmParams& p, const LaunchCfg& cfg) {
   auto kern = k_assemble<D, P, FORM, KP1, LOADM, CT>;
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    configured = true;
-  }
+  static unsigned long long configured = 0;
+  allow_dynamic_smem(kern, configured);
   const auto& cb = *cfg.class_begin;
   for (size_t k = 0; k + 1 < cb.size(); ++k) {
     const int n = cb[k + 1] - cb[k];
