@@ -100,7 +100,14 @@ def emit_assign(lines, name, expr):
         if e.is_Symbol:
             return str(e)
         if e.is_Add:
-            return "(" + " + ".join(rec(a) for a in e.args) + ")"
+            text = ""
+            for a in e.args:
+                c, _ = a.as_coeff_Mul()
+                if c < 0:
+                    text = f"{text} - {rec(-a)}" if text else f"-{rec(-a)}"
+                else:
+                    text = f"{text} + {rec(a)}" if text else rec(a)
+            return "(" + text + ")"
         if e.is_Mul:
             return "(" + " * ".join(rec(a) for a in e.args) + ")"
         if e.is_Pow and e.exp == 2:
@@ -165,31 +172,103 @@ def load_kappa_text(name, d, p, kind):
     return "\n".join(lines)
 
 
+def _rational_gcd(values):
+    """Largest rational g with every value / g an integer."""
+    from math import gcd
+    num, den = 0, 1
+    for v in values:
+        v = sp.Rational(v)
+        if v == 0:
+            continue
+        num = gcd(num, abs(int(v.p)))
+        den = den * int(v.q) // gcd(den, int(v.q))
+    return sp.Rational(num, den) if num else sp.Integer(1)
+
+
+def _int_coeffs(expr):
+    return [sp.Rational(c) for c in sp.Poly(expr, *sorted(expr.free_symbols, key=str)).coeffs()] \
+        if expr.free_symbols else [sp.Rational(expr)]
+
+
 def function_text(name, d, p, kind, with_kappa):
+    """Row function in scaled form.  With s = NAME_scale (the largest rational
+    that divides every reference-tensor coefficient of the row), the caller
+    passes W' = s W and the function returns the row; every coefficient left
+    is a small integer, so each output is an FMA chain over the W' entries
+    (one multiply of an integer-weight kappa combination per term) and one
+    final integer factor."""
     outs, na = gen_grad_grad(d, p, kind, with_kappa)
     nb = d + 1
     nj = len(outs)
+    Wsyms = [sp.Symbol(f"W[{ia}][{b}]") for ia in range(na) for b in range(nb)]
+    coeffs = []
+    for e in outs:
+        e = sp.expand(e)
+        if e != 0:
+            coeffs += _int_coeffs(e)
+    sigma = _rational_gcd(coeffs)
+    # per output: integer factor g_j and the terms W * q(kappa), q with
+    # coprime integer coefficients
+    rows = []
+    for e in outs:
+        e = sp.expand(e / sigma)
+        if e == 0:
+            rows.append((0, []))
+            continue
+        g = _rational_gcd(_int_coeffs(e))
+        e = sp.expand(e / g)
+        terms = []
+        for w in Wsyms:
+            q = sp.expand(e.coeff(w))
+            if q != 0:
+                terms.append((w, q))
+        rows.append((g, terms))
     args = f"const CT (&W)[{na}][{nb}]"
     if with_kappa:
         args += f", const CT (&kap)[{nb}]"
     args += f", CT (&out)[{nj}]"
     lines = [
+        f"constexpr double {name}_scale = {float(sigma)!r};  // {sigma}",
         "template <typename CT>",
         f"DB2_HD void {name}({args}) {{",
     ]
-    # common subexpressions over the whole row
-    repl, reduced = sp.cse(outs, symbols=sp.numbered_symbols("t"), optimizations="basic")
-    for sym, e in repl:
-        lines.append(f"  const CT {sym} = 0;")
-        lines.pop()
-        tmp = []
-        emit_assign(tmp, f"const CT {sym}", e)
-        lines.extend(tmp)
-    for j, e in enumerate(reduced):
-        if e == 0:
-            lines.append(f"  out[{j}] = CT(0);")
+    # common kappa combinations over the whole row
+    qs = [q for _, terms in rows for _, q in terms if q.free_symbols]
+    uniq = list(dict.fromkeys(qs))
+    repl, reduced = sp.cse(uniq, symbols=sp.numbered_symbols("t"), optimizations="basic")
+    for sym, ex in repl:
+        emit_assign(lines, f"const CT {sym}", ex)
+    qname = {}
+    for k, (q, r) in enumerate(zip(uniq, reduced)):
+        if r.is_Symbol:
+            qname[q] = str(r)
         else:
-            emit_assign(lines, f"out[{j}]", e)
+            emit_assign(lines, f"const CT q{k}", r)
+            qname[q] = f"q{k}"
+
+    def factor(q):
+        if q.free_symbols:
+            return qname[q]
+        return lit(q)
+
+    for j, (g, terms) in enumerate(rows):
+        if not terms:
+            lines.append(f"  out[{j}] = CT(0);")
+            continue
+        w0, q0 = terms[0]
+        acc = f"{w0} * {factor(q0)}" if q0 != 1 else f"{w0}"
+        if q0 == -1:
+            acc = f"-{w0}"
+        for w, q in terms[1:]:
+            if q == 1:
+                acc = f"({acc} + {w})"
+            elif q == -1:
+                acc = f"({acc} - {w})"
+            else:
+                acc = f"fma({w}, {factor(q)}, {acc})"
+        if g != 1:
+            acc = f"{lit(g)} * ({acc})"
+        lines.append(f"  out[{j}] = {acc};")
     lines.append("}")
     return "\n".join(lines), nj, na
 
@@ -216,10 +295,12 @@ def main():
         "// vertex 0; row 'e': the row of the edge (0,1).  Columns follow the UFC local",
         "// node order of the (relabelled) cell: vertices, then edges in the order of",
         "// TetrahedronCell/TriangleCell::create_entities.",
-        "//   grad_grad_*_k1 : out_j = sum_ab W_ab (1/|T|) int dphi_i/dl_a dphi_j/dl_b",
+        "//   grad_grad_*_k1 : out_j = sum_ab W_ab (1/|T|) int dphi_i/dl_a dphi_j/dl_b,",
+        "//                    called with W * grad_grad_*_scale (integer coefficients remain)",
         "//   grad_grad_*_kp1: same with a P1 weight kappa = sum_k kap_k l_k inside",
         "//   load_*_f1      : (1/|T|) int phi_i ;  load_*_fp1: (1/|T|) int f phi_i",
         "#pragma once",
+        "#include <cmath>",
         "#ifndef DB2_HD",
         "#if defined(__CUDACC__)",
         "#define DB2_HD __host__ __device__ __forceinline__",

@@ -80,10 +80,12 @@ __global__ void __launch_bounds__(256) k_vjp_cells(const AsmParams p, int64_t nc
     for (int j = 0; j < E::K; ++j) g[j] = __ldg(grow + rr.slot(j));
     CT W0[1][NB];
     CT W1[2][NB];
-    for (int b = 0; b < NB; ++b) W0[0][b] = CT(ndot<D>(G, 0, b) * (G.s * p.kscale));
+    // W times the generated rows' scale (see element_rows.h)
+    for (int b = 0; b < NB; ++b) W0[0][b] = CT(ndot<D>(G, 0, b) * (G.s * (p.kscale * R::sv_kp1)));
     if constexpr (P == 2)
       for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < NB; ++b) W1[a][b] = CT(ndot<D>(G, a, b) * (G.s * p.kscale));
+        for (int b = 0; b < NB; ++b)
+          W1[a][b] = CT(ndot<D>(G, a, b) * (G.s * (p.kscale * R::se_kp1)));
     double fv[NB];
     if constexpr (LOADK)
       for (int a = 0; a < NB; ++a) fv[a] = __ldg(p.f + pv[a]);

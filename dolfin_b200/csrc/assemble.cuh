@@ -182,6 +182,8 @@ struct Rows;
 #define DB2_ROWS(D_, P_, NAME, K_)                                                          \
   template <typename CT>                                                                   \
   struct Rows<D_, P_, CT> {                                                                \
+    static constexpr double sv_k1 = gen::grad_grad_##NAME##_v_k1_scale;                    \
+    static constexpr double sv_kp1 = gen::grad_grad_##NAME##_v_kp1_scale;                  \
     __device__ static void v_k1(const CT (&W)[1][D_ + 1], CT (&o)[K_]) {                    \
       gen::grad_grad_##NAME##_v_k1<CT>(W, o);                                               \
     }                                                                                      \
@@ -197,6 +199,8 @@ struct Rows;
       gen::load_##NAME##_v_kfp1<CT>(f, o);                                                  \
     }
 #define DB2_ROWS_EDGE(D_, NAME, K_)                                                         \
+  static constexpr double se_k1 = gen::grad_grad_##NAME##_e_k1_scale;                      \
+  static constexpr double se_kp1 = gen::grad_grad_##NAME##_e_kp1_scale;                    \
   __device__ static void e_k1(const CT (&W)[2][D_ + 1], CT (&o)[K_]) {                      \
     gen::grad_grad_##NAME##_e_k1<CT>(W, o);                                                 \
   }                                                                                        \
@@ -406,9 +410,14 @@ __device__ __forceinline__ void element_row(const AsmParams& p, const Geometry<D
 #pragma unroll
     for (int a = 0; a < NB; ++a) kc[a] = CT(kap[a]);
   }
+  // the generated rows take W times their scale (integer coefficients remain)
+  double sig = KP1 ? R::sv_kp1 : R::sv_k1;
+  if constexpr (P == 2) {
+    if (!vertex) sig = KP1 ? R::se_kp1 : R::se_k1;
+  }
   auto wval = [&](int a, int b) -> double {
     if constexpr (FORM == FORM_DIFF) {
-      return ndot<D>(G, a, b) * (G.s * p.kscale);
+      return ndot<D>(G, a, b) * (G.s * (p.kscale * sig));
     } else {
       double nac = G.n[a][0], nae = G.n[a][0], nbc = G.n[b][0], nbe = G.n[b][0];
 #pragma unroll
@@ -418,7 +427,7 @@ __device__ __forceinline__ void element_row(const AsmParams& p, const Geometry<D
       }
       double w = p.lmbda * nac * nbe + p.mu * nae * nbc;
       if (c == e) w = fma(p.mu, ndot<D>(G, a, b), w);
-      return G.s * w;
+      return (G.s * sig) * w;
     }
   };
   if (P == 1 || vertex) {
@@ -507,8 +516,14 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
     const int jstar = vertex ? 0 : E::K - 1;
     double diag = 0.0;
     uint32_t dslot = 0;
+    // the next record is fetched one incidence ahead: its load (the head of
+    // the dependent chain record -> vertex records -> geometry) overlaps the
+    // current incidence's arithmetic
+    Rec<D, P> rn{};
+    if (cnt > 0) rn = load_rec<D, P>(p, rbase);
     for (uint32_t m = 0; m < cnt; ++m) {
-      const Rec<D, P> r = load_rec<D, P>(p, rbase + 32u * m);
+      const Rec<D, P> r = rn;
+      if (m + 1 < cnt) rn = load_rec<D, P>(p, rbase + 32u * (m + 1));
       double x[D + 1][D], kap[D + 1], fv[D + 1];
       record_cell<D, P, FP1>(p, F, r, x, kap, fv);
       Geometry<D> G;
@@ -566,16 +581,25 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
   __syncthreads();
 }
 
-// Three resident 256-thread blocks per SM caps registers at 85 per thread:
-// the heaviest instantiations spill at most 60 bytes (to L1), and 128-thread
-// tiles run 6 CTAs (24 warps) per SM instead of 3-4.  The kernel is latency
-// bound, so the extra warps win (P2 tets at n=96: 1.84 ms against 2.08 ms
-// with 142 registers).
-#ifndef DB2_TILE_MIN_BLOCKS
-#define DB2_TILE_MIN_BLOCKS 3
+// Resident 256-thread blocks per SM that the launch bounds guarantee, which
+// caps registers per thread (65536 / (256 x blocks)).  The kernel is latency
+// bound, so warps per SM matter, but the P2 rows keep up to 15 kappa
+// combinations and W' entries live across their FMA chains; measured on
+// B200, two blocks (128 registers) beat three (85 registers, with spills):
+// P2 tets n=96 1.71 ms against 1.83 ms, vector P2 elasticity n=48 1.56 ms
+// against 1.83 ms, P1 tets n=32 0.041 ms against 0.045 ms.
+#ifndef DB2_TILE_MIN_BLOCKS_P1
+#define DB2_TILE_MIN_BLOCKS_P1 2
 #endif
+#ifndef DB2_TILE_MIN_BLOCKS_P2
+#define DB2_TILE_MIN_BLOCKS_P2 2
+#endif
+template <int P>
+constexpr int tile_min_blocks() {
+  return P == 1 ? DB2_TILE_MIN_BLOCKS_P1 : DB2_TILE_MIN_BLOCKS_P2;
+}
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
-__global__ void __launch_bounds__(kMaxTileThreads, DB2_TILE_MIN_BLOCKS) k_assemble(const AsmParams p) {
+__global__ void __launch_bounds__(kMaxTileThreads, tile_min_blocks<P>()) k_assemble(const AsmParams p) {
   extern __shared__ double acc[];
   tile_body<D, P, FORM, KP1, LOADM, CT>(p, p.tiles[blockIdx.x], acc);
 }
