@@ -244,6 +244,21 @@ def algorithmic_bytes(w):
     return csr_bytes(A.nnz(), V.dim(), C, k_node, 3, Nv, Nv * len(w["fields"]), True)
 
 
+def profiled_traffic(workload):
+    """DRAM bytes (read + write) per step of the assembly kernels, from the
+    committed ncu launch list of this workload (profiles/); None if there is
+    none.  It is a separate one-pass ncu capture, not measured by this run."""
+    path = os.path.join(ROOT, "profiles", f"k_assemble_launches_{workload}.txt")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_step:"):
+                    return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def sustain(fn, seconds):
     """Run fn() back to back for about `seconds` (clock sampling window)."""
     import torch
@@ -547,7 +562,8 @@ def main():
                        "l2": "flushed between steps (256 MiB write)", "setup_s": round(w["setup_s"], 2),
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": profiled_traffic(args.workload),
                          "peak_source": peak_kind, "algorithmic_bytes": B},
             "fp32_contract": {"value": round(cells / (ms32 * 1e-3) / 1e6, 3), "unit": "Mcells/s",
                               "ms_per_step": round(ms32, 4), "speedup_vs_fp64": round(ms_step / ms32, 3),
