@@ -375,6 +375,41 @@ __device__ __forceinline__ RowFix<D> load_row_fix(const AsmParams& p, uint32_t n
   return r;
 }
 
+// Same with the kind of row known at compile time (NFIX fixed vertices).
+template <int D, int P, bool FP1, int NFIX>
+__device__ __forceinline__ RowFix<D> load_row_fix_n(const AsmParams& p, uint32_t node) {
+  RowFix<D> r;
+  r.nfix = NFIX;
+  if constexpr (NFIX == 1) {
+    r.base = node;
+    load_vertex<D, FP1>(p, node, r.x[0], r.kap[0], r.f[0]);
+  } else {
+    const uint2 e = __ldg(reinterpret_cast<const uint2*>(p.edge_v) + (node - p.nverts));
+    r.base = e.x;
+    load_vertex<D, FP1>(p, e.x, r.x[0], r.kap[0], r.f[0]);
+    load_vertex<D, FP1>(p, e.y, r.x[1], r.kap[1], r.f[1]);
+  }
+  return r;
+}
+
+template <int D, int P, bool FP1, int NFIX>
+__device__ __forceinline__ void record_cell_n(const AsmParams& p, const RowFix<D>& F,
+                                              const Rec<D, P>& r, double (&x)[D + 1][D],
+                                              double (&kap)[D + 1], double (&fv)[D + 1]) {
+#pragma unroll
+  for (int a = 0; a <= D; ++a) {
+    if (a < NFIX) {
+#pragma unroll
+      for (int q = 0; q < D; ++q) x[a][q] = F.x[a][q];
+      kap[a] = F.kap[a];
+      fv[a] = F.f[a];
+    } else {
+      const uint32_t v = uint32_t(int32_t(F.base) + r.delta(a - NFIX));
+      load_vertex<D, FP1>(p, v, x[a], kap[a], fv[a]);
+    }
+  }
+}
+
 // The relabelled cell of one record: fixed vertices first, then the others.
 template <int D, int P, bool FP1>
 __device__ __forceinline__ void record_cell(const AsmParams& p, const RowFix<D>& F,
@@ -415,17 +450,26 @@ __device__ __forceinline__ void element_row(const AsmParams& p, const Geometry<D
   if constexpr (P == 2) {
     if (!vertex) sig = KP1 ? R::se_kp1 : R::se_k1;
   }
+  // elasticity: components c and e of every cofactor vector, selected once
+  // per incidence rather than inside each entry of W^{ce}
+  double nc[NB], ne[NB];
+  if constexpr (FORM == FORM_ELAS) {
+#pragma unroll
+    for (int a = 0; a < NB; ++a) {
+      nc[a] = G.n[a][0];
+      ne[a] = G.n[a][0];
+#pragma unroll
+      for (int r = 1; r < D; ++r) {
+        if (c == r) nc[a] = G.n[a][r];
+        if (e == r) ne[a] = G.n[a][r];
+      }
+    }
+  }
   auto wval = [&](int a, int b) -> double {
     if constexpr (FORM == FORM_DIFF) {
       return ndot<D>(G, a, b) * (G.s * (p.kscale * sig));
     } else {
-      double nac = G.n[a][0], nae = G.n[a][0], nbc = G.n[b][0], nbe = G.n[b][0];
-#pragma unroll
-      for (int r = 1; r < D; ++r) {
-        if (c == r) { nac = G.n[a][r]; nbc = G.n[b][r]; }
-        if (e == r) { nae = G.n[a][r]; nbe = G.n[b][r]; }
-      }
-      double w = p.lmbda * nac * nbe + p.mu * nae * nbc;
+      double w = p.lmbda * nc[a] * ne[b] + p.mu * ne[a] * nc[b];
       if (c == e) w = fma(p.mu, ndot<D>(G, a, b), w);
       return (G.s * sig) * w;
     }
@@ -469,6 +513,85 @@ __device__ __forceinline__ double load_row(const AsmParams& p, const Geometry<D>
 }
 
 
+// One row unit (node row, trial block e) of a tile whose rows are all vertex
+// nodes (NFIX = 1 fixed vertex) or all edge nodes (NFIX = 2).
+template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int NFIX>
+__device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, double* acc,
+                                         double* bpart, int32_t r0, int u) {
+  using E = El<D, P>;
+  constexpr int BS = FORM == FORM_ELAS ? D : 1;
+  constexpr bool FP1 = LOADM == LOAD_P1;
+  constexpr bool vertex = NFIX == 1;
+  const bool bc = p.bc_flags != nullptr;
+  const uint32_t node = t.n0 + u / BS;
+  const int e = u % BS;
+  const int32_t ra = __ldg(p.node_rowptr + node);
+  const int32_t L = __ldg(p.node_rowptr + node + 1) - ra;
+  double* my = acc + BS * (ra - r0) + e * L;
+  const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - __ldg(p.inc_ptr + node);
+  const uint32_t rbase = __ldg(p.rec_goff + (node >> 5)) + (node & 31u);
+  double bsum = 0.0;
+  const int64_t rowdof = int64_t(t.comp) * p.nnodes + node;
+  bool row_bc = false;
+  double row_g = 0.0;
+  const int32_t* colrow = nullptr;
+  if (bc) {
+    row_bc = __ldg(p.bc_flags + rowdof) != 0;
+    row_g = row_bc ? __ldg(p.bc_vals + rowdof) : 0.0;
+    colrow = p.cols + int64_t(t.comp) * BS * p.nnz_node + int64_t(BS) * ra + e * L;
+  }
+  const RowFix<D> F = load_row_fix_n<D, P, FP1, NFIX>(p, node);
+  // the row node is relabelled local node 0 (vertex) or K-1 (edge (0,1));
+  // its column is the same for every incidence: accumulate it in a register
+  constexpr int jstar = vertex ? 0 : E::K - 1;
+  double diag = 0.0;
+  uint32_t dslot = 0;
+  // the next record is fetched one incidence ahead: its load (the head of
+  // the dependent chain record -> vertex records -> geometry) overlaps the
+  // current incidence's arithmetic
+  Rec<D, P> rn{};
+  if (cnt > 0) rn = load_rec<D, P>(p, rbase);
+  for (uint32_t m = 0; m < cnt; ++m) {
+    const Rec<D, P> r = rn;
+    if (m + 1 < cnt) rn = load_rec<D, P>(p, rbase + 32u * (m + 1));
+    double x[D + 1][D], kap[D + 1], fv[D + 1];
+    record_cell_n<D, P, FP1, NFIX>(p, F, r, x, kap, fv);
+    Geometry<D> G;
+    geometry(x, G);
+    CT out[E::K];
+    element_row<D, P, FORM, KP1, CT>(p, G, vertex, t.comp, e, kap, out);
+    if constexpr (LOADM != LOAD_NONE) {
+      if (e == 0) bsum += load_row<D, P, LOADM>(p, G, vertex, t.comp, fv);
+    }
+    if (bc) {
+      if (row_bc) {
+#pragma unroll
+        for (int j = 0; j < E::K; ++j) out[j] = CT((e == t.comp && j == jstar) ? 1 : 0);
+        if constexpr (LOADM != LOAD_NONE) {
+          if (e == 0) bsum = bsum - load_row<D, P, LOADM>(p, G, vertex, t.comp, fv) + row_g;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < E::K; ++j) {
+          const int32_t dof = __ldg(colrow + r.slot(j));
+          if (__ldg(p.bc_flags + dof)) {
+            bsum -= double(out[j]) * __ldg(p.bc_vals + dof);
+            out[j] = CT(0);
+          }
+        }
+      }
+    }
+    dslot = r.slot(jstar);
+#pragma unroll
+    for (int j = 0; j < E::K; ++j) {
+      if (j == jstar) diag += double(out[j]);
+      else my[r.slot(j)] += double(out[j]);
+    }
+  }
+  if (cnt) my[dslot] += diag;
+  bpart[u] = bsum;
+}
+
 // One tile: rows [t.n0, t.n1) of test component t.comp.  `acc` holds the
 // tile's CSR value segment followed by one double per row unit (load-vector
 // partials).  blockDim must be at least the tile's unit count.
@@ -480,86 +603,20 @@ __device__ __forceinline__ double load_row(const AsmParams& p, const Geometry<D>
 // and zero them.
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
 __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, double* acc) {
-  using E = El<D, P>;
   constexpr int BS = FORM == FORM_ELAS ? D : 1;
-  constexpr bool FP1 = LOADM == LOAD_P1;
   const int32_t r0 = __ldg(p.node_rowptr + t.n0), r1 = __ldg(p.node_rowptr + t.n1);
   const int seg = BS * (r1 - r0);
   double* bpart = acc + seg;
   for (int i = threadIdx.x; i < seg; i += blockDim.x) acc[i] = 0.0;
   __syncthreads();
   const int units = (t.n1 - t.n0) * BS;
-  const bool bc = p.bc_flags != nullptr;
   if (int(threadIdx.x) < units) {
-    const int u = threadIdx.x;
-    const uint32_t node = t.n0 + u / BS;
-    const int e = u % BS;
-    const int32_t ra = __ldg(p.node_rowptr + node);
-    const int32_t L = __ldg(p.node_rowptr + node + 1) - ra;
-    double* my = acc + BS * (ra - r0) + e * L;
-    const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - __ldg(p.inc_ptr + node);
-    const uint32_t rbase = __ldg(p.rec_goff + (node >> 5)) + (node & 31u);
-    double bsum = 0.0;
-    const int64_t rowdof = int64_t(t.comp) * p.nnodes + node;
-    bool row_bc = false;
-    double row_g = 0.0;
-    const int32_t* colrow = nullptr;
-    if (bc) {
-      row_bc = __ldg(p.bc_flags + rowdof) != 0;
-      row_g = row_bc ? __ldg(p.bc_vals + rowdof) : 0.0;
-      colrow = p.cols + int64_t(t.comp) * BS * p.nnz_node + int64_t(BS) * ra + e * L;
-    }
-    const RowFix<D> F = load_row_fix<D, P, FP1>(p, node);
-    const bool vertex = F.nfix == 1;
-    // the row node is relabelled local node 0 (vertex) or K-1 (edge (0,1));
-    // its column is the same for every incidence: accumulate it in a register
-    const int jstar = vertex ? 0 : E::K - 1;
-    double diag = 0.0;
-    uint32_t dslot = 0;
-    // the next record is fetched one incidence ahead: its load (the head of
-    // the dependent chain record -> vertex records -> geometry) overlaps the
-    // current incidence's arithmetic
-    Rec<D, P> rn{};
-    if (cnt > 0) rn = load_rec<D, P>(p, rbase);
-    for (uint32_t m = 0; m < cnt; ++m) {
-      const Rec<D, P> r = rn;
-      if (m + 1 < cnt) rn = load_rec<D, P>(p, rbase + 32u * (m + 1));
-      double x[D + 1][D], kap[D + 1], fv[D + 1];
-      record_cell<D, P, FP1>(p, F, r, x, kap, fv);
-      Geometry<D> G;
-      geometry(x, G);
-      CT out[E::K];
-      element_row<D, P, FORM, KP1, CT>(p, G, vertex, t.comp, e, kap, out);
-      if constexpr (LOADM != LOAD_NONE) {
-        if (e == 0) bsum += load_row<D, P, LOADM>(p, G, vertex, t.comp, fv);
-      }
-      if (bc) {
-        if (row_bc) {
-#pragma unroll
-          for (int j = 0; j < E::K; ++j) out[j] = CT((e == t.comp && j == jstar) ? 1 : 0);
-          if constexpr (LOADM != LOAD_NONE) {
-            if (e == 0) bsum = bsum - load_row<D, P, LOADM>(p, G, vertex, t.comp, fv) + row_g;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < E::K; ++j) {
-            const int32_t dof = __ldg(colrow + r.slot(j));
-            if (__ldg(p.bc_flags + dof)) {
-              bsum -= double(out[j]) * __ldg(p.bc_vals + dof);
-              out[j] = CT(0);
-            }
-          }
-        }
-      }
-      dslot = r.slot(jstar);
-#pragma unroll
-      for (int j = 0; j < E::K; ++j) {
-        if (j == jstar) diag += double(out[j]);
-        else my[r.slot(j)] += double(out[j]);
-      }
-    }
-    if (cnt) my[dslot] += diag;
-    bpart[u] = bsum;
+    // tiles never mix vertex and edge nodes (the host cuts P2 tiles at the
+    // first edge node), so the row kind is uniform over the block
+    if (P == 1 || t.n0 < p.nverts)
+      row_unit<D, P, FORM, KP1, LOADM, CT, 1>(p, t, acc, bpart, r0, int(threadIdx.x));
+    else if constexpr (P == 2)
+      row_unit<D, P, FORM, KP1, LOADM, CT, 2>(p, t, acc, bpart, r0, int(threadIdx.x));
   }
   __syncthreads();
   if constexpr (LOADM != LOAD_NONE) {

@@ -296,12 +296,16 @@ void canonical_node_map(int tdim, int degree, int li, int* map) {
 std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doubles, int* max_seg_out) {
   const int bs = P.bs;
   const int64_t nn = P.V->nnodes;
+  // P2: vertex nodes [0, nv) precede edge nodes; no tile spans both, so the
+  // kernel knows each tile's row kind up front
+  const int64_t split = P.V->degree == 2 ? P.V->mesh->nv : -1;
   int max_seg = 0;
   std::vector<Tile> comp0;
   int64_t n0 = 0;
   while (n0 < nn) {
     int64_t n1 = n0;
     while (n1 < nn) {
+      if (n1 == split && n1 > n0) break;
       const int64_t units = (n1 + 1 - n0) * bs;
       const int64_t seg = int64_t(bs) * (P.node_rowptr[n1 + 1] - P.node_rowptr[n0]);
       if (units > tile_threads || seg > seg_cap_doubles) break;
