@@ -36,9 +36,17 @@ WORKLOADS = {
     "elasticity_p2_48": ("elasticity", 48, 2, "vector P2 elasticity, UnitCubeMesh(48) jittered 0.15h, A+b"),
     "poisson_p1_32": ("poisson", 32, 1, "P1 Poisson kappa P1 + load f P1, UnitCubeMesh(32), A+b"),
     "poisson_p2_96": ("poisson", 96, 2, "P2 Poisson kappa P1 + load f P1, UnitCubeMesh(96), A+b"),
+    "poisson_p1_64": ("poisson", 64, 1, "P1 Poisson kappa=exp(g) g~N(0,0.25) + load f P1, "
+                      "UnitCubeMesh(64), A+b; adjoint dL/dkappa timed beside it"),
+    "poisson_p1_96": ("poisson", 96, 1, "P1 Poisson kappa=exp(g) g~N(0,0.25) + load f P1, "
+                      "UnitCubeMesh(96), A+b; adjoint dL/dkappa timed beside it"),
     "batched_512": ("batched", 512, 0, "512 UnitSquareMesh(n), n log-uniform [8,256], jitter 0.2h, "
                     "P1/P2 kappa*grad.grad, one graph-captured persistent launch"),
 }
+
+
+# the adjoint workloads: kappa = exp(g), g ~ N(0, 0.5^2) per vertex
+LOGNORMAL_KAPPA = {"poisson_p1_64", "poisson_p1_96"}
 
 
 def run_batched(args, rank, world):
@@ -54,8 +62,7 @@ def run_batched(args, rank, world):
     for V, _ in members:
         V.pattern()
     setup_s = time.perf_counter() - t0
-    best, timings = autotune(members, precision="fp64",
-                             cache_path=os.path.join(ROOT, "_work", "tune_cache.json") if os.path.isdir(os.path.join(ROOT, "_work")) else None)
+    best, timings = autotune(members, precision="fp64", cache_path=None)
     B = BatchAssembler(members, *best)
     cells = B.ncells
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -212,7 +219,10 @@ def setup_workload(name, seed, device):
         x = x0
         V = d2.FunctionSpace(mesh, "Lagrange", deg)
         W = d2.FunctionSpace(mesh, "Lagrange", 1)
-        kv = synthetic.uniform_field(mesh.num_vertices(), 0.5, 2.0, seed)
+        if name in LOGNORMAL_KAPPA:
+            kv = synthetic.lognormal_field(mesh.num_vertices(), 0.5, seed)
+        else:
+            kv = synthetic.uniform_field(mesh.num_vertices(), 0.5, 2.0, seed)
         fv = synthetic.uniform_field(mesh.num_vertices(), -1.0, 1.0, seed + 1)
         kappa, f = d2.Function(W, kv), d2.Function(W, fv)
         u, v = d2.TrialFunction(V), d2.TestFunction(V)
@@ -326,10 +336,30 @@ def cpu_baseline_sample(w, target_s=10.0, threads=1):
 _REF = {}
 
 
-def _ref_init(workload, rank, ncells):
+def _ref_init(workload, rank, ncells, ncores):
+    """Oracle inputs of one reference worker: `ncells` consecutive cells of the
+    workload mesh (3D workloads), or whole member meshes of the batched
+    workload taken round-robin until about `ncells` cells."""
     from oracle import oracle as orc
     from dolfin_b200 import synthetic
     kind, n, deg, _ = WORKLOADS[workload]
+    if kind == "batched":
+        jobs, done = [], 0
+        specs = synthetic.batched_square_meshes(512, 2024)
+        for sp in specs[rank::ncores]:
+            m = sp["n"]
+            om = orc.unit_square_mesh(m, m)
+            om.coords = synthetic.jitter_interior(om.coords, m, sp["jitter"], sp["seed"])
+            kv = synthetic.uniform_field(om.nv, 0.5, 2.0, sp["seed"] + 1)
+            od, N = orc.dofmap(om, sp["degree"], 1)
+            rp, cols = orc.sparsity(N, N, od, od)
+            fa = orc.form(orc.DIFFUSION, 2, sp["degree"], 1, coeff=orc.COEFF_P1)
+            jobs.append((fa, om, od, rp, cols, kv))
+            done += om.nc
+            if done >= ncells:
+                break
+        _REF.update(orc=orc, jobs=jobs, ncells=done)
+        return
     om = orc.unit_cube_mesh(n, n, n)
     vs = 3 if kind == "elasticity" else 1
     if kind == "elasticity":
@@ -340,27 +370,33 @@ def _ref_init(workload, rank, ncells):
     else:
         fa = orc.form(orc.DIFFUSION, 3, deg, 1, coeff=orc.COEFF_P1)
         fl = orc.form(orc.LOAD, 3, deg, 1, coeff=orc.COEFF_P1)
-        wa = synthetic.uniform_field(om.nv, 0.5, 2.0, 1000)
+        wa = (synthetic.lognormal_field(om.nv, 0.5, 1000) if workload in LOGNORMAL_KAPPA
+              else synthetic.uniform_field(om.nv, 0.5, 2.0, 1000))
         wl = synthetic.uniform_field(om.nv, -1.0, 1.0, 1001)
     od, N = orc.dofmap(om, deg, vs)
     lo = (rank * ncells) % om.nc
     sub = orc.Mesh(3, om.coords, np.ascontiguousarray(om.cells[lo:lo + ncells]))
     dsub = np.ascontiguousarray(od[lo:lo + ncells])
     rp, cols = orc.sparsity(N, N, dsub, dsub)
-    _REF.update(orc=orc, sub=sub, dsub=dsub, rp=rp, cols=cols, fa=fa, fl=fl, wa=wa, wl=wl, N=N)
+    _REF.update(orc=orc, sub=sub, dsub=dsub, rp=rp, cols=cols, fa=fa, fl=fl, wa=wa, wl=wl, N=N,
+                jobs=None, ncells=sub.nc)
 
 
 def _ref_work(_):
     r = _REF
     t0 = time.perf_counter()
-    r["orc"].assemble_matrix(r["fa"], r["sub"], r["dsub"], r["dsub"], r["rp"], r["cols"], w=r["wa"])
-    r["orc"].assemble_vector(r["fl"], r["sub"], r["dsub"], r["N"], w=r["wl"])
+    if r["jobs"] is not None:
+        for fa, om, od, rp, cols, kv in r["jobs"]:
+            r["orc"].assemble_matrix(fa, om, od, od, rp, cols, w=kv)
+    else:
+        r["orc"].assemble_matrix(r["fa"], r["sub"], r["dsub"], r["dsub"], r["rp"], r["cols"], w=r["wa"])
+        r["orc"].assemble_vector(r["fl"], r["sub"], r["dsub"], r["N"], w=r["wl"])
     return time.perf_counter() - t0
 
 
-def _ref_worker_main(workload, rank, ncells, steps, warmup, q_in, q_out):
-    _ref_init(workload, rank, ncells)
-    q_out.put("ready")
+def _ref_worker_main(workload, rank, ncells, ncores, q_in, q_out):
+    _ref_init(workload, rank, ncells, ncores)
+    q_out.put(("ready", _REF["ncells"]))
     while True:
         msg = q_in.get()
         if msg is None:
@@ -375,17 +411,20 @@ def run_reference(args, rank, world):
     ctx = mp.get_context("spawn")
     kind, n, deg, desc = WORKLOADS[args.workload]
     ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    per = {"elasticity": 512, "poisson": 32768 if deg == 1 else 4096}[kind]
+    per = {"elasticity": 512, "poisson": 32768 if deg == 1 else 4096, "batched": 16384}[kind]
     procs, qin, qout = [], [], []
     for r in range(ncores):
         qi, qo = ctx.Queue(), ctx.Queue()
-        p = ctx.Process(target=_ref_worker_main, args=(args.workload, r, per, args.steps, args.warmup, qi, qo))
+        p = ctx.Process(target=_ref_worker_main, args=(args.workload, r, per, ncores, qi, qo))
         p.start()
         procs.append(p)
         qin.append(qi)
         qout.append(qo)
+    cells_per_step = 0
     for qo in qout:
-        assert qo.get(timeout=900) == "ready"
+        tag, nc = qo.get(timeout=900)
+        assert tag == "ready"
+        cells_per_step += nc
 
     def step():
         t0 = time.perf_counter()
@@ -403,7 +442,7 @@ def run_reference(args, rank, world):
     for p in procs:
         p.join(timeout=60)
     t = float(np.mean(times))
-    value = ncores * per / t / 1e6
+    value = cells_per_step / t / 1e6
     line = {
         "metric": METRIC, "impl": "reference", "value": round(value, 4), "unit": "Mcells/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -411,8 +450,11 @@ def run_reference(args, rank, world):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; same mesh and fields)",
         "config": {"workload": args.workload, "description": desc},
         "cpu_baseline": {"value": round(value, 4), "unit": "Mcells/s", "cores": ncores, "kind": "port",
-                         "sample": f"{per} cells per core x {ncores} cores per step (disjoint ranges), "
-                                   "oracle restatement of DOLFIN's serial assemble_cells + EigenMatrix::add"},
+                         "sample": (f"{cells_per_step} cells per step over {ncores} cores "
+                                    + ("(whole member meshes, round-robin)" if kind == "batched"
+                                       else "(disjoint cell ranges)")
+                                    + ", oracle restatement of DOLFIN's serial assemble_cells + "
+                                      "EigenMatrix::add")},
         "e2e": {"value": round(value, 4), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -512,6 +554,20 @@ def main():
         d2.assemble_action(w["a"], d2.Vector(x), y)
     ms_mf = float(np.mean(time_steps(lambda: d2.assemble_action(w["a"], d2.Vector(x), y), args.steps, flush)))
 
+    # adjoint of L(kappa) = <gA, A(kappa)> with respect to the P1 kappa
+    vjp = None
+    if w["kind"] == "poisson":
+        from dolfin_b200.autodiff import vjp_kappa
+        kt = torch.as_tensor(w["fields"]["kappa"], device="cuda")
+        gA = torch.randn(A.nnz(), dtype=torch.float64, device="cuda",
+                         generator=torch.Generator("cuda").manual_seed(11))
+        for _ in range(args.warmup):
+            vjp_kappa(w["V"], kt, gA)
+        ms_vjp = float(np.mean(time_steps(lambda: vjp_kappa(w["V"], kt, gA), args.steps, flush)))
+        vjp = {"ms_per_call": round(ms_vjp, 4), "ratio_to_forward_step": round(ms_vjp / ms_step, 3),
+               "what": "dL/dkappa of L = <gA, A(kappa)>, gA ~ N(0,1) over the CSR values"}
+        del gA
+
     # end to end through the public API with host buffers: per step, H2D of the
     # step's input (vertex coordinates for elasticity, kappa and f otherwise)
     # and D2H of the result (CSR values and b)
@@ -577,6 +633,8 @@ def main():
             "clocks": clk.summary(),
             "wall_s_timed_region": round(t_wall, 3),
         }
+        if vjp is not None:
+            line["vjp"] = vjp
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
