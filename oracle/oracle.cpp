@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <stdexcept>
 #include <vector>
@@ -195,10 +196,14 @@ int coeff_degree(int coeff) {
 
 int form_rank(int kind) {
   switch (kind) {
-    case ORC_LOAD: return 1;
-    case ORC_FUNCTIONAL: return 0;
+    case ORC_LOAD: case ORC_FACET_LOAD: return 1;
+    case ORC_FUNCTIONAL: case ORC_FACET_FUNCTIONAL: return 0;
     default: return 2;
   }
+}
+
+bool is_facet_kind(int kind) {
+  return kind == ORC_FACET_MASS || kind == ORC_FACET_LOAD || kind == ORC_FACET_FUNCTIONAL;
 }
 
 int quadrature_degree(const orc_form& f) {
@@ -211,6 +216,8 @@ int quadrature_degree(const orc_form& f) {
     case ORC_ELASTICITY: return p0 + p1 - 2;
     case ORC_DIV_P: return p0 - 1 + p1;
     case ORC_GRADP_V: return p0 + p1 - 1;
+    case ORC_FACET_MASS: return p0 + p1 + c;
+    case ORC_FACET_LOAD: return p0 + c;
     default: return c;
   }
 }
@@ -297,8 +304,9 @@ struct Tabulator {
         return s;
       }
       case ORC_COEFF_X0: {
+        const int comp = (int)f.c[1];
         double s = 0.0;
-        for (int a = 0; a <= d; ++a) s += xc[a * d] * l[a];
+        for (int a = 0; a <= d; ++a) s += xc[a * d + comp] * l[a];
         return s;
       }
       case ORC_COEFF_P1_TIMES_P1: {
@@ -391,6 +399,157 @@ struct Tabulator {
     }
   }
 };
+
+// Exterior facet integrals (ufc::exterior_facet_integral::tabulate_tensor,
+// FFC-generated; called at Assembler.cpp:277-281): the facet tensor in the
+// cell's local dof layout, integrated exactly with a Gauss--Jacobi rule on the
+// reference facet mapped into the cell.  Local facet f is opposite local
+// vertex f; its points have cell barycentrics lambda_f = 0 and lambda_{a_k} =
+// mu_k for the facet's vertices a_0 < a_1 (< a_2).  The physical measure is
+// |F| (d-1)! times the reference facet weight.
+struct FacetTabulator {
+  orc_form f;
+  Quadrature q;
+  int k0 = 0, k1 = 0, n0 = 0, n1 = 0;
+  // per local facet: basis values and cell barycentrics at the points
+  std::vector<double> phi0[4], phi1[4], lam[4];
+
+  explicit FacetTabulator(const orc_form& form) : f(form) {
+    const int d = f.tdim;
+    q = make_quadrature(d - 1, quadrature_degree(f));
+    const int rank = form_rank(f.kind);
+    if (rank >= 1) { k0 = scalar_dim(f.family0, f.degree0, d); n0 = k0 * f.vsize0; }
+    if (rank == 2) { k1 = scalar_dim(f.family1, f.degree1, d); n1 = k1 * f.vsize1; }
+    const int np = q.size();
+    std::vector<double> dummy(30 * 3);
+    for (int fl = 0; fl <= d; ++fl) {
+      int av[3], m = 0;
+      for (int a = 0; a <= d; ++a)
+        if (a != fl) av[m++] = a;
+      phi0[fl].resize(np * std::max(k0, 1));
+      phi1[fl].resize(np * std::max(k1, 1));
+      lam[fl].resize(np * (d + 1));
+      for (int p = 0; p < np; ++p) {
+        double mu[3], s = 0.0;
+        for (int r = 0; r < d - 1; ++r) { mu[r + 1] = q.X[p * (d - 1) + r]; s += mu[r + 1]; }
+        mu[0] = 1.0 - s;
+        double l[4] = {0, 0, 0, 0};
+        for (int k = 0; k < d; ++k) l[av[k]] = mu[k];
+        double X[3];
+        for (int r = 0; r < d; ++r) X[r] = l[r + 1];
+        for (int a = 0; a <= d; ++a) lam[fl][p * (d + 1) + a] = l[a];
+        if (k0) eval_basis(f.family0, f.degree0, d, X, &phi0[fl][p * k0], dummy.data());
+        if (k1) eval_basis(f.family1, f.degree1, d, X, &phi1[fl][p * k1], dummy.data());
+      }
+    }
+  }
+
+  // |F| (d-1)!: the facet's length (2D) or twice its area (3D)
+  static double measure_factor(int d, const double* xc, int fl) {
+    int av[3], m = 0;
+    for (int a = 0; a <= d; ++a)
+      if (a != fl) av[m++] = a;
+    if (d == 2) {
+      const double dx = xc[av[1] * 2] - xc[av[0] * 2], dy = xc[av[1] * 2 + 1] - xc[av[0] * 2 + 1];
+      return std::sqrt(dx * dx + dy * dy);
+    }
+    double u[3], v[3];
+    for (int r = 0; r < 3; ++r) {
+      u[r] = xc[av[1] * 3 + r] - xc[av[0] * 3 + r];
+      v[r] = xc[av[2] * 3 + r] - xc[av[0] * 3 + r];
+    }
+    const double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2],
+                 cz = u[0] * v[1] - u[1] * v[0];
+    return std::sqrt(cx * cx + cy * cy + cz * cz);
+  }
+
+  void tabulate(const double* xc, const double* w, int fl, double* A) const {
+    const int d = f.tdim;
+    const int rank = form_rank(f.kind);
+    const int size = rank == 2 ? n0 * n1 : (rank == 1 ? n0 : 1);
+    std::fill(A, A + size, 0.0);
+    const double scale = measure_factor(d, xc, fl);
+    for (int p = 0; p < q.size(); ++p) {
+      const double* l = &lam[fl][p * (d + 1)];
+      double kq = 1.0;
+      if (f.coeff == ORC_COEFF_CONST) kq = f.c[0];
+      else if (f.coeff == ORC_COEFF_P1) {
+        kq = 0.0;
+        for (int a = 0; a <= d; ++a) kq += w[a] * l[a];
+      } else if (f.coeff == ORC_COEFF_X0) {
+        const int comp = (int)f.c[1];
+        kq = 0.0;
+        for (int a = 0; a <= d; ++a) kq += xc[a * d + comp] * l[a];
+      }
+      const double wq = q.w[p] * scale;
+      const double* ph0 = &phi0[fl][p * std::max(k0, 1)];
+      const double* ph1 = &phi1[fl][p * std::max(k1, 1)];
+      switch (f.kind) {
+        case ORC_FACET_MASS:
+          for (int i = 0; i < k0; ++i)
+            for (int j = 0; j < k1; ++j) A[i * n1 + j] += wq * kq * ph0[i] * ph1[j];
+          break;
+        case ORC_FACET_LOAD:
+          if (f.vsize0 == 1) {
+            for (int i = 0; i < k0; ++i) A[i] += wq * kq * ph0[i];
+          } else {
+            for (int c = 0; c < f.vsize0; ++c)
+              for (int i = 0; i < k0; ++i) A[c * k0 + i] += wq * f.c[c] * ph0[i];
+          }
+          break;
+        case ORC_FACET_FUNCTIONAL:
+          A[0] += wq * kq;
+          break;
+        default:
+          throw std::runtime_error("not a facet form");
+      }
+    }
+  }
+};
+
+// Facet::exterior() (one incident cell) over the facets numbered by
+// TopologyComputation::compute_entities_by_key_matching
+// (dolfin/mesh/TopologyComputation.cpp:152-330): sorted vertex keys, in key
+// order.  Cell facet i is opposite local vertex i
+// (TetrahedronCell::create_entities / TriangleCell::create_entities).
+struct ExtFacets {
+  std::vector<uint32_t> cell;
+  std::vector<int32_t> local;
+};
+
+ExtFacets exterior_facets(int d, int64_t nc, const uint32_t* cells) {
+  struct Keyed { uint32_t k[3]; int64_t slot; };
+  const int nf = d + 1;
+  std::vector<Keyed> keyed((size_t)nc * nf);
+  for (int64_t c = 0; c < nc; ++c)
+    for (int fl = 0; fl < nf; ++fl) {
+      Keyed& K = keyed[c * nf + fl];
+      int m = 0;
+      for (int a = 0; a <= d; ++a)
+        if (a != fl) K.k[m++] = cells[c * nf + a];
+      for (; m < 3; ++m) K.k[m] = 0;
+      std::sort(K.k, K.k + d);
+      K.slot = c * nf + fl;
+    }
+  auto less = [](const Keyed& x, const Keyed& y) {
+    for (int r = 0; r < 3; ++r)
+      if (x.k[r] != y.k[r]) return x.k[r] < y.k[r];
+    return x.slot < y.slot;
+  };
+  std::sort(keyed.begin(), keyed.end(), less);
+  ExtFacets E;
+  size_t i = 0;
+  while (i < keyed.size()) {
+    size_t j = i + 1;
+    while (j < keyed.size() && std::equal(keyed[j].k, keyed[j].k + 3, keyed[i].k)) ++j;
+    if (j - i == 1) {
+      E.cell.push_back((uint32_t)(keyed[i].slot / nf));
+      E.local.push_back((int32_t)(keyed[i].slot % nf));
+    }
+    i = j;
+  }
+  return E;
+}
 
 // Cell::get_coordinate_dofs (dolfin/mesh/Cell.h:293-307): vertex-major copy.
 void gather_coordinates(int d, const double* coords, const uint32_t* cell, double* xc) {
@@ -665,8 +824,29 @@ int orc_assemble_matrix(const orc_form* f, int64_t nv, const double* coords, int
                         const double* w, const double* w2, int64_t nrows, const int32_t* rowptr,
                         const int32_t* cols, double* vals, int add_values) {
   (void)nv;
-  Tabulator t(*f);
   const int d = f->tdim;
+  if (is_facet_kind(f->kind)) {
+    // Assembler::assemble_exterior_facets (dolfin/fem/Assembler.cpp:196-288)
+    FacetTabulator t(*f);
+    if (!add_values) std::fill(vals, vals + rowptr[nrows], 0.0);
+    const ExtFacets E = exterior_facets(d, nc, cells);
+    std::vector<double> A((size_t)t.n0 * t.n1);
+    double xc[12], wc[4];
+    for (size_t i = 0; i < E.cell.size(); ++i) {
+      const int64_t c = E.cell[i];
+      const uint32_t* cell = cells + c * (d + 1);
+      gather_coordinates(d, coords, cell, xc);
+      gather_vertex_field(d, w, cell, wc);
+      t.tabulate(xc, wc, E.local[i], A.data());
+      const int32_t* r = dofs0 + c * t.n0;
+      const int32_t* cc = dofs1 + c * t.n1;
+      for (int a = 0; a < t.n0; ++a)
+        for (int b = 0; b < t.n1; ++b)
+          if (!csr_add(rowptr, cols, vals, r[a], cc[b], A[a * t.n1 + b])) return -2;
+    }
+    return 0;
+  }
+  Tabulator t(*f);
   if (!add_values) std::fill(vals, vals + rowptr[nrows], 0.0);
   std::vector<double> A((size_t)t.n0 * t.n1);
   double xc[12], wc[4], wc2[4];
@@ -691,8 +871,25 @@ int orc_assemble_vector(const orc_form* f, int64_t nv, const double* coords, int
                         const uint32_t* cells, const int32_t* dofs0, const double* w,
                         const double* w2, int64_t n, double* b, int add_values) {
   (void)nv;
-  Tabulator t(*f);
   const int d = f->tdim;
+  if (is_facet_kind(f->kind)) {
+    FacetTabulator t(*f);
+    if (!add_values) std::fill(b, b + n, 0.0);
+    const ExtFacets E = exterior_facets(d, nc, cells);
+    std::vector<double> be(t.n0);
+    double xc[12], wc[4];
+    for (size_t i = 0; i < E.cell.size(); ++i) {
+      const int64_t c = E.cell[i];
+      const uint32_t* cell = cells + c * (d + 1);
+      gather_coordinates(d, coords, cell, xc);
+      gather_vertex_field(d, w, cell, wc);
+      t.tabulate(xc, wc, E.local[i], be.data());
+      const int32_t* r = dofs0 + c * t.n0;
+      for (int a = 0; a < t.n0; ++a) b[r[a]] += be[a];
+    }
+    return 0;
+  }
+  Tabulator t(*f);
   if (!add_values) std::fill(b, b + n, 0.0);
   std::vector<double> be(t.n0);
   double xc[12], wc[4], wc2[4];
@@ -712,8 +909,21 @@ int orc_assemble_vector(const orc_form* f, int64_t nv, const double* coords, int
 double orc_assemble_scalar(const orc_form* f, int64_t nv, const double* coords, int64_t nc,
                            const uint32_t* cells, const double* w) {
   (void)nv;
-  Tabulator t(*f);
   const int d = f->tdim;
+  if (is_facet_kind(f->kind)) {
+    FacetTabulator t(*f);
+    const ExtFacets E = exterior_facets(d, nc, cells);
+    double s = 0.0, a = 0.0, xc[12], wc[4];
+    for (size_t i = 0; i < E.cell.size(); ++i) {
+      const uint32_t* cell = cells + (int64_t)E.cell[i] * (d + 1);
+      gather_coordinates(d, coords, cell, xc);
+      gather_vertex_field(d, w, cell, wc);
+      t.tabulate(xc, wc, E.local[i], &a);
+      s += a;
+    }
+    return s;
+  }
+  Tabulator t(*f);
   double s = 0.0, a = 0.0, xc[12], wc[4];
   for (int64_t c = 0; c < nc; ++c) {
     const uint32_t* cell = cells + c * (d + 1);
@@ -735,15 +945,36 @@ int orc_assemble_system(const orc_form* a, const orc_form* L, int64_t nv, const 
                         const double* wa, const double* wL, int64_t nbc, const int32_t* bc_dofs,
                         const double* bc_vals, int64_t n, const int32_t* rowptr,
                         const int32_t* cols, double* vals, double* b) {
+  return orc_assemble_system_ds(a, nullptr, L, nullptr, nv, coords, nc, cells, dofs, wa, nullptr,
+                                wL, nullptr, nbc, bc_dofs, bc_vals, n, rowptr, cols, vals, b);
+}
+
+int orc_assemble_system_ds(const orc_form* a, const orc_form* a_ds, const orc_form* L,
+                           const orc_form* L_ds, int64_t nv, const double* coords, int64_t nc,
+                           const uint32_t* cells, const int32_t* dofs, const double* wa,
+                           const double* wa_ds, const double* wL, const double* wL_ds,
+                           int64_t nbc, const int32_t* bc_dofs, const double* bc_vals, int64_t n,
+                           const int32_t* rowptr, const int32_t* cols, double* vals, double* b) {
   (void)nv;
   Tabulator ta(*a), tL(*L);
   const int d = a->tdim;
   if (ta.n0 != ta.n1 || ta.n0 != tL.n0) return -1;
   const int k = ta.n0;
+  std::unique_ptr<FacetTabulator> tfa, tfL;
+  if (a_ds) tfa.reset(new FacetTabulator(*a_ds));
+  if (L_ds) tfL.reset(new FacetTabulator(*L_ds));
+  if ((tfa && (tfa->n0 != k || tfa->n1 != k)) || (tfL && tfL->n0 != k)) return -1;
+  // exterior flag of each (cell, local facet)
+  std::vector<uint8_t> ext;
+  if (tfa || tfL) {
+    ext.assign((size_t)nc * (d + 1), 0);
+    const ExtFacets E = exterior_facets(d, nc, cells);
+    for (size_t i = 0; i < E.cell.size(); ++i) ext[(size_t)E.cell[i] * (d + 1) + E.local[i]] = 1;
+  }
   std::fill(vals, vals + rowptr[n], 0.0);
   std::fill(b, b + n, 0.0);
-  std::vector<double> Ae((size_t)k * k), be(k);
-  double xc[12], wc[4], wcL[4];
+  std::vector<double> Ae((size_t)k * k), be(k), Af((size_t)k * k), bf(k);
+  double xc[12], wc[4], wcL[4], wcf[4];
   auto bc_lookup = [&](int32_t dof, double& v) {
     const int32_t* it = std::lower_bound(bc_dofs, bc_dofs + nbc, dof);
     if (it == bc_dofs + nbc || *it != dof) return false;
@@ -757,6 +988,21 @@ int orc_assemble_system(const orc_form* a, const orc_form* L, int64_t nv, const 
     gather_vertex_field(d, wL, cell, wcL);
     ta.tabulate(xc, wc, wc, Ae.data());
     tL.tabulate(xc, wcL, wcL, be.data());
+    // exterior facets of the cell, in local facet order
+    if (!ext.empty())
+      for (int fl = 0; fl <= d; ++fl) {
+        if (!ext[(size_t)c * (d + 1) + fl]) continue;
+        if (tfa) {
+          gather_vertex_field(d, wa_ds, cell, wcf);
+          tfa->tabulate(xc, wcf, fl, Af.data());
+          for (int i = 0; i < k * k; ++i) Ae[i] += Af[i];
+        }
+        if (tfL) {
+          gather_vertex_field(d, wL_ds, cell, wcf);
+          tfL->tabulate(xc, wcf, fl, bf.data());
+          for (int i = 0; i < k; ++i) be[i] += bf[i];
+        }
+      }
     const int32_t* cd = dofs + c * k;
     for (int i = 0; i < k; ++i) {
       double g;
@@ -774,6 +1020,16 @@ int orc_assemble_system(const orc_form* a, const orc_form* L, int64_t nv, const 
     }
   }
   return 0;
+}
+
+int64_t orc_exterior_facets(int tdim, int64_t nc, const uint32_t* cells, uint32_t* facet_cell,
+                            int32_t* facet_local) {
+  const ExtFacets E = exterior_facets(tdim, nc, cells);
+  for (size_t i = 0; i < E.cell.size(); ++i) {
+    if (facet_cell) facet_cell[i] = E.cell[i];
+    if (facet_local) facet_local[i] = E.local[i];
+  }
+  return (int64_t)E.cell.size();
 }
 
 int64_t orc_boundary_vertices(int gdim, int64_t nv, const double* coords, int32_t* out) {

@@ -33,14 +33,18 @@ enum orc_form_kind {
                           sigma = 2 mu eps + lmbda tr(eps) I                  */
   ORC_DIV_P = 5,       /* a = div(v) * p * dx     (v vector test, p trial)    */
   ORC_GRADP_V = 6,     /* a = inner(grad(p), v) * dx                          */
-  ORC_FUNCTIONAL = 7   /* M = coeff * dx, coeff = const, P1 field or x[0]     */
+  ORC_FUNCTIONAL = 7,  /* M = coeff * dx, coeff = const, P1 field or x[i]     */
+  /* exterior facet integrals (Assembler::assemble_exterior_facets)           */
+  ORC_FACET_MASS = 8,       /* a = coeff * u * v * ds   (scalar spaces)       */
+  ORC_FACET_LOAD = 9,       /* L = coeff * v * ds, or inner(c, v) * ds        */
+  ORC_FACET_FUNCTIONAL = 10 /* M = coeff * ds                                 */
 };
 
 enum orc_coeff_kind {
   ORC_COEFF_NONE = 0,   /* coefficient == 1                                   */
   ORC_COEFF_CONST = 1,  /* Constant: value(s) in c[]                          */
   ORC_COEFF_P1 = 2,     /* P1 Function given by its vertex values             */
-  ORC_COEFF_X0 = 3,     /* SpatialCoordinate x[0]                             */
+  ORC_COEFF_X0 = 3,     /* SpatialCoordinate x[i], i = (int)c[1] (0 default)  */
   ORC_COEFF_P1_TIMES_P1 = 4 /* product of two P1 fields (w, w2)               */
 };
 
@@ -72,6 +76,13 @@ int orc_interval_mesh(int n, double* coords, uint32_t* cells);
    edge_vertices[ne*2]. */
 int64_t orc_edges(int tdim, int64_t nc, const uint32_t* cells,
                   uint32_t* cell_edges, uint32_t* edge_vertices);
+
+/* Exterior facets (facets with one incident cell), in facet-number order
+   (key order, as compute_entities_by_key_matching numbers them): the cell of
+   each and its local facet index (facet i is opposite local vertex i).
+   Arrays hold up to nc*(tdim+1) entries; returns the count. */
+int64_t orc_exterior_facets(int tdim, int64_t nc, const uint32_t* cells,
+                            uint32_t* facet_cell, int32_t* facet_local);
 
 /* ---- dofmap (DofMapBuilder::build with reorder_dofs_serial = false) --- */
 /* Returns the global dimension; fills cell_dofs[nc * ndofs_per_cell]. */
@@ -120,6 +131,17 @@ int orc_assemble_system(const orc_form* a, const orc_form* L, int64_t nv,
                         int64_t nbc, const int32_t* bc_dofs, const double* bc_vals,
                         int64_t n, const int32_t* rowptr, const int32_t* cols,
                         double* vals, double* b);
+
+/* Same with exterior facet integrals a_ds / L_ds (either may be NULL) added
+   to each cell tensor before apply_bc, as SystemAssembler::cell_wise_assembly
+   does for the exterior facets of the cell (SystemAssembler.cpp:417-470). */
+int orc_assemble_system_ds(const orc_form* a, const orc_form* a_ds, const orc_form* L,
+                           const orc_form* L_ds, int64_t nv, const double* coords,
+                           int64_t nc, const uint32_t* cells, const int32_t* dofs,
+                           const double* wa, const double* wa_ds, const double* wL,
+                           const double* wL_ds, int64_t nbc, const int32_t* bc_dofs,
+                           const double* bc_vals, int64_t n, const int32_t* rowptr,
+                           const int32_t* cols, double* vals, double* b);
 
 /* Vertices on the boundary of a UnitCube/UnitSquare box mesh (the dofs of
    DirichletBC(V, g, "on_boundary") for P1); returns count. */

@@ -21,6 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
 DIFFUSION, MASS, LOAD, ELASTICITY, DIV_P, GRADP_V, FUNCTIONAL = 1, 2, 3, 4, 5, 6, 7
+FACET_MASS, FACET_LOAD, FACET_FUNCTIONAL = 8, 9, 10
 COEFF_NONE, COEFF_CONST, COEFF_P1, COEFF_X0, COEFF_P1_TIMES_P1 = 0, 1, 2, 3, 4
 CG, DG = 0, 1
 
@@ -68,6 +69,10 @@ def lib():
         L.orc_assemble_scalar.argtypes = [P, i64, P, i64, P, P]
         L.orc_assemble_scalar.restype = C.c_double
         L.orc_assemble_system.argtypes = [P, P, i64, P, i64, P, P, P, P, i64, P, P, i64, P, P, P, P]
+        L.orc_assemble_system_ds.argtypes = [P, P, P, P, i64, P, i64, P, P, P, P, P, P, i64, P, P,
+                                             i64, P, P, P, P]
+        L.orc_exterior_facets.argtypes = [i32, i64, P, P, P]
+        L.orc_exterior_facets.restype = i64
         L.orc_boundary_vertices.argtypes = [i32, i64, P, P]
         L.orc_boundary_vertices.restype = i64
         L.orc_vjp_diffusion.argtypes = [P, i64, P, i64, P, P, P, P, P, P, P, i32, P]
@@ -218,6 +223,36 @@ def assemble_system(a, L, mesh, dofs, n, rowptr, cols, bc_dofs, bc_vals, wa=None
     if rc != 0:
         raise RuntimeError(f"oracle assemble_system failed ({rc})")
     return vals, b
+
+
+def assemble_system_ds(a, L, mesh, dofs, n, rowptr, cols, bc_dofs, bc_vals, wa=None, wL=None,
+                       a_ds=None, L_ds=None, wa_ds=None, wL_ds=None):
+    """SystemAssembler with exterior facet integrals a_ds / L_ds (or None)."""
+    vals = np.zeros(cols.shape[0], np.float64)
+    b = np.zeros(n, np.float64)
+    coords = np.ascontiguousarray(mesh.coords, np.float64)
+    cells = np.ascontiguousarray(mesh.cells, np.uint32)
+    bc_dofs = np.ascontiguousarray(bc_dofs, np.int32)
+    bc_vals = np.ascontiguousarray(bc_vals, np.float64)
+    ref = lambda f: None if f is None else C.byref(f)
+    rc = lib().orc_assemble_system_ds(C.byref(a), ref(a_ds), C.byref(L), ref(L_ds), mesh.nv,
+                                      _p(coords), mesh.nc, _p(cells),
+                                      _p(np.ascontiguousarray(dofs, np.int32)), _p(wa), _p(wa_ds),
+                                      _p(wL), _p(wL_ds), bc_dofs.shape[0], _p(bc_dofs),
+                                      _p(bc_vals), n, _p(rowptr), _p(cols), _p(vals), _p(b))
+    if rc != 0:
+        raise RuntimeError(f"oracle assemble_system_ds failed ({rc})")
+    return vals, b
+
+
+def exterior_facets(mesh):
+    """(cell, local facet) of each exterior facet, in facet-number order."""
+    cells = np.ascontiguousarray(mesh.cells, np.uint32)
+    cap = mesh.nc * (mesh.tdim + 1)
+    fc = np.empty(cap, np.uint32)
+    fl = np.empty(cap, np.int32)
+    m = lib().orc_exterior_facets(mesh.tdim, mesh.nc, _p(cells), _p(fc), _p(fl))
+    return fc[:m].copy(), fl[:m].copy()
 
 
 def boundary_vertices(mesh):

@@ -151,3 +151,65 @@ def test_edge_numbering_key_order(orc):
     for c in range(m.nc):
         for e, (p, q) in enumerate(tet):
             assert tuple(ev[ce[c, e]]) == (m.cells[c, p], m.cells[c, q])
+
+
+@pytest.mark.parametrize("mesh,area", [("square", 4.0), ("cube", 6.0)])
+def test_facet_functional_area(orc, mesh, area):
+    # python/test/unit/fem/test_assembler.py:140-153: assemble(1*ds(mesh)) is
+    # the boundary measure: 4.0 on UnitSquareMesh(4, 4), 6.0 on UnitCubeMesh(2, 2, 2).
+    m = orc.unit_square_mesh(4, 4) if mesh == "square" else orc.unit_cube_mesh(2, 2, 2)
+    f = orc.form(orc.FACET_FUNCTIONAL, m.tdim, coeff=orc.COEFF_CONST, c=(1.0,))
+    assert round(orc.assemble_scalar(f, m) - area, 7) == 0
+
+
+@pytest.mark.parametrize("tdim,n", [(2, 5), (3, 3)])
+def test_exterior_facets(orc, tdim, n):
+    # boundary facets of the box mesh: 4n edges (2D), 2 per boundary square (3D);
+    # numbered in sorted-key order, each opposite the listed local vertex
+    m = orc.unit_square_mesh(n, n) if tdim == 2 else orc.unit_cube_mesh(n, n, n)
+    fc, fl = orc.exterior_facets(m)
+    assert fc.shape[0] == (4 * n if tdim == 2 else 12 * n * n)
+    keys = [tuple(sorted(np.delete(m.cells[c], f).tolist())) for c, f in zip(fc, fl)]
+    assert keys == sorted(keys) and len(set(keys)) == len(keys)
+    x = m.coords
+    for c, f in zip(fc, fl):
+        pts = x[np.delete(m.cells[c], f)]
+        assert np.any(np.all(np.isclose(pts, 0.0), axis=0) | np.all(np.isclose(pts, 1.0), axis=0))
+
+
+@pytest.mark.parametrize("deg", [1, 2])
+@pytest.mark.parametrize("tdim", [2, 3])
+def test_facet_integral_identities(orc, tdim, deg):
+    # sum_i int_dO g phi_i = g |dO|;  1^T M_ds 1 = |dO|;  int_dO x_i ds = |dO| / 2
+    n = 4 if tdim == 2 else 2
+    m = orc.unit_square_mesh(n, n) if tdim == 2 else orc.unit_cube_mesh(n, n, n)
+    area = 4.0 if tdim == 2 else 6.0
+    d, N = orc.dofmap(m, deg)
+    b = orc.assemble_vector(orc.form(orc.FACET_LOAD, tdim, deg, coeff=orc.COEFF_CONST, c=(2.5,)),
+                            m, d, N)
+    assert abs(b.sum() - 2.5 * area) < 1e-12
+    rp, cols = orc.sparsity(N, N, d, d)
+    M = orc.assemble_matrix(orc.form(orc.FACET_MASS, tdim, deg), m, d, d, rp, cols)
+    assert abs(M.sum() - area) < 1e-12
+    for comp in range(tdim):
+        fx = orc.form(orc.FACET_FUNCTIONAL, tdim, coeff=orc.COEFF_X0, c=(0.0, comp))
+        assert abs(orc.assemble_scalar(fx, m) - area / 2) < 1e-12
+
+
+def test_system_with_facets_without_bcs(orc):
+    # with no Dirichlet dofs the cell-wise system is the sum of the cell and
+    # exterior-facet assemblies
+    m = orc.unit_cube_mesh(2, 2, 2)
+    d, N = orc.dofmap(m, 2)
+    rp, cols = orc.sparsity(N, N, d, d)
+    kv = np.linspace(0.5, 2.0, m.nv)
+    a = orc.form(orc.DIFFUSION, 3, 2, coeff=orc.COEFF_P1)
+    a_ds = orc.form(orc.FACET_MASS, 3, 2, coeff=orc.COEFF_CONST, c=(3.0,))
+    L = orc.form(orc.LOAD, 3, 2, coeff=orc.COEFF_CONST, c=(1.0,))
+    L_ds = orc.form(orc.FACET_LOAD, 3, 2, coeff=orc.COEFF_P1)
+    vals, b = orc.assemble_system_ds(a, L, m, d, N, rp, cols, np.zeros(0, np.int32), np.zeros(0),
+                                     wa=kv, a_ds=a_ds, L_ds=L_ds, wL_ds=kv)
+    A1 = orc.assemble_matrix(a, m, d, d, rp, cols, w=kv) + orc.assemble_matrix(a_ds, m, d, d, rp, cols)
+    b1 = orc.assemble_vector(L, m, d, N) + orc.assemble_vector(L_ds, m, d, N, w=kv)
+    assert np.max(np.abs(vals - A1)) < 1e-13 * np.max(np.abs(A1))
+    assert np.max(np.abs(b - b1)) < 1e-13 * np.max(np.abs(b1))
