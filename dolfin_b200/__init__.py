@@ -20,15 +20,15 @@ from .cpp import (DofMap, FunctionSpace, Mesh, SparsityPattern, UnitCubeMesh, Un
                   VectorFunctionSpace, parameters)
 from .function import Constant, Function
 from .la import Matrix, Vector
-from .ufl import (Identity, TestFunction, TrialFunction, div, dot, dx, grad, inner, nabla_grad,
-                  sym, tr, transpose)
+from .ufl import (Identity, SpatialCoordinate, TestFunction, TrialFunction, div, dot, ds, dx, grad,
+                  inner, nabla_grad, sym, tr, transpose)
 
 __all__ = [
     "assemble", "assemble_system", "assemble_action", "SystemAssembler", "Mesh", "UnitCubeMesh",
     "UnitSquareMesh", "FunctionSpace", "VectorFunctionSpace", "DofMap", "SparsityPattern",
     "parameters", "Function", "Constant", "Matrix", "Vector", "TestFunction", "TrialFunction",
-    "grad", "inner", "dot", "dx", "div", "sym", "tr", "transpose", "nabla_grad", "Identity",
-    "DirichletBC",
+    "grad", "inner", "dot", "dx", "ds", "div", "sym", "tr", "transpose", "nabla_grad", "Identity",
+    "DirichletBC", "SpatialCoordinate",
 ]
 
 

@@ -17,7 +17,8 @@ ERR_NAMES = {1: "argument", 2: "shape", 3: "index", 4: "mesh", 5: "unsupported",
              7: "out of memory", 8: "timeout"}
 
 FORM_DIFFUSION, FORM_LOAD, FORM_ELASTICITY = 1, 2, 3
-COEFF_NONE, COEFF_CONSTANT, COEFF_P1, COEFF_P1_SCALED = 0, 1, 2, 3
+FORM_FACET_MASS, FORM_FACET_LOAD, FORM_FUNCTIONAL, FORM_FACET_FUNCTIONAL = 4, 5, 6, 7
+COEFF_NONE, COEFF_CONSTANT, COEFF_P1, COEFF_P1_SCALED, COEFF_COORD = 0, 1, 2, 3, 4
 FP64, FP32_CONTRACT = 0, 1
 
 
@@ -50,6 +51,8 @@ _SIGS = {
     "db2_mesh_copy": [P, P, P],
     "db2_mesh_set_coordinates": [P, P],
     "db2_mesh_num_edges": [P, C.POINTER(I64)],
+    "db2_mesh_num_exterior_facets": [P, C.POINTER(I64)],
+    "db2_mesh_exterior_facets": [P, P, P],
     "db2_mesh_destroy": [P],
     "db2_space_create": [P, I, I, PP],
     "db2_space_info": [P, C.POINTER(I), C.POINTER(I64)],
@@ -63,11 +66,15 @@ _SIGS = {
                               C.POINTER(I64), C.POINTER(I64)],
     "db2_pattern_plan_copy": [P, P, P, P, P, P, P],
     "db2_pattern_retile": [P, I, I],
+    "db2_pattern_facet_plan_info": [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I)],
+    "db2_pattern_facet_plan_copy": [P, P, P, P, P],
     "db2_pattern_destroy": [P],
     "db2_assemble_matrix": [P, P, P, I, P, I, P],
     "db2_assemble_vector": [P, P, P, P, I, P],
     "db2_assemble_system": [P, P, P, P, P, I, P, P, P],
     "db2_assemble_system_bc": [P, P, P, P, P, P, P, I, P, P, P],
+    "db2_assemble_scalar": [P, P, P, P, P],
+    "db2_assemble_facets_bc": [P, P, P, P, P, P, P, P, P, P],
     "db2_apply": [P, P, P, I, P, P, P],
     "db2_vjp_kappa": [P, P, P, P, P, P, P, I, P, P],
     "db2_vjp_kappa_noalloc": [P, P, P, P, P, P, P, I, P, P],

@@ -16,7 +16,7 @@ import ctypes as C
 from . import _capi
 from ._capi import call
 from .la import Matrix, Vector
-from .ufl import Form, recognise
+from .ufl import Form, Recognised, recognise, recognise_functional, recognise_parts
 
 _PREC = {"fp64": _capi.FP64, "fp32": _capi.FP32_CONTRACT, None: _capi.FP64}
 
@@ -47,14 +47,21 @@ def _check_tensor_dims(tensor, rec):
 
 def assemble(form, tensor=None, form_compiler_parameters=None, add_values=False,
              finalize_tensor=True, keep_diagonal=False, backend=None, precision="fp64"):
-    """Assemble a bilinear or linear form on the GPU (dolfin.assemble)."""
+    """Assemble a form on the GPU (dolfin.assemble): a Matrix for bilinear, a
+    Vector for linear forms, a float for functionals.  dx terms run the cell
+    kernels, ds terms then add the exterior-facet contributions (the
+    reference's cell loop, then exterior-facet loop, Assembler.cpp:52-103)."""
     if backend is not None:
         raise NotImplementedError("only the default backend (device CSR) is provided")
     if not isinstance(form, Form):
         raise TypeError("expected a Form")
-    rec = recognise(form)
+    if form.rank() == 0:
+        return _assemble_scalar(form)
+    cell, facet = recognise_parts(form)
+    rec = cell or facet
     prec = _PREC[precision]
-    if rec.kind in (_capi.FORM_DIFFUSION, _capi.FORM_ELASTICITY):
+    parts = [r for r in (cell, facet) if r is not None]
+    if form.rank() == 2:
         A = tensor if tensor is not None else Matrix()
         if A.empty():
             A.init(rec.V.pattern(keep_diagonal))
@@ -62,15 +69,35 @@ def assemble(form, tensor=None, form_compiler_parameters=None, add_values=False,
             _check_tensor_dims(A, rec)
             if A.pattern.V is not rec.V:
                 raise RuntimeError("*** Error: tensor pattern belongs to another function space")
-        call("db2_assemble_matrix", A.pattern.handle, C.byref(rec.c_form()), _coeff_ptr(rec), prec,
-             _ptr(A.values_tensor()), int(bool(add_values)), _stream())
+        for i, r in enumerate(parts):
+            call("db2_assemble_matrix", A.pattern.handle, C.byref(r.c_form()), _coeff_ptr(r), prec,
+                 _ptr(A.values_tensor()), int(bool(add_values) or i > 0), _stream())
         return A
     b = tensor if tensor is not None else Vector(n=rec.V.dim())
     if b.size() != rec.V.dim():
         raise RuntimeError("*** Error: Unable to assemble form. Reason: Dim 0 of tensor does not match form.")
-    call("db2_assemble_vector", rec.V.pattern(keep_diagonal).handle, C.byref(rec.c_form()),
-         _coeff_ptr(rec), _ptr(b.tensor()), int(bool(add_values)), _stream())
+    for i, r in enumerate(parts):
+        call("db2_assemble_vector", rec.V.pattern(keep_diagonal).handle, C.byref(r.c_form()),
+             _coeff_ptr(r), _ptr(b.tensor()), int(bool(add_values) or i > 0), _stream())
     return b
+
+
+def _assemble_scalar(form):
+    """double assemble(const Form&) (dolfin/fem/assemble.h:66): the sum of
+    the dx and ds parts, each reduced on the device in a fixed order."""
+    import torch
+    total = 0.0
+    for kind, mesh, coeff, func, const in recognise_functional(form):
+        w = None
+        if func is not None:
+            if func.function_space().mesh() is not mesh:
+                raise ValueError("coefficient and form live on different meshes")
+            w = _ptr(func.tensor())
+        out = torch.empty(1, dtype=torch.float64, device="cuda")
+        call("db2_assemble_scalar", mesh.handle, C.byref(_capi.make_form(kind, coeff, const)), w,
+             _ptr(out), _stream())
+        total += float(out.item())
+    return total
 
 
 class SystemAssembler:
@@ -78,7 +105,14 @@ class SystemAssembler:
     (dolfin/fem/SystemAssembler.cpp:138-301, cell_wise_assembly :303-492)."""
 
     def __init__(self, a, L, bcs=None, precision="fp64"):
-        self.ra, self.rL = recognise(a), recognise(L)
+        self.ra, self.ra_ds = recognise_parts(a)
+        self.rL, self.rL_ds = recognise_parts(L)
+        if self.ra is None:
+            raise NotImplementedError("the bilinear form needs a cell (dx) part")
+        if self.rL is None:
+            # L has only ds terms: the cell pass assembles a zero load
+            self.rL = Recognised(_capi.FORM_LOAD, self.ra.V, _capi.COEFF_CONSTANT, None,
+                                 (0.0, 0.0, 0.0))
         if self.ra.V is not self.rL.V:
             raise RuntimeError("a and L must share the function space")
         self.bcs = [] if bcs is None else (bcs if isinstance(bcs, (list, tuple)) else [bcs])
@@ -100,15 +134,33 @@ class SystemAssembler:
             call("db2_assemble_system_bc", A.pattern.handle, C.byref(self.ra.c_form()),
                  _coeff_ptr(self.ra), C.byref(self.rL.c_form()), _coeff_ptr(self.rL), _ptr(flags),
                  _ptr(vals), self.prec, _ptr(A.values_tensor()), _ptr(b.tensor()), _stream())
+            if self.ra_ds is not None or self.rL_ds is not None:
+                # exterior-facet terms with the same Dirichlet treatment
+                fa = C.byref(self.ra_ds.c_form()) if self.ra_ds is not None else None
+                fl = C.byref(self.rL_ds.c_form()) if self.rL_ds is not None else None
+                call("db2_assemble_facets_bc", A.pattern.handle, fa,
+                     _coeff_ptr(self.ra_ds) if self.ra_ds is not None else None, fl,
+                     _coeff_ptr(self.rL_ds) if self.rL_ds is not None else None, _ptr(flags),
+                     _ptr(vals), _ptr(A.values_tensor()), _ptr(b.tensor()), _stream())
         else:
             call("db2_assemble_system", A.pattern.handle, C.byref(self.ra.c_form()),
                  _coeff_ptr(self.ra), C.byref(self.rL.c_form()), _coeff_ptr(self.rL), self.prec,
                  _ptr(A.values_tensor()), _ptr(b.tensor()), _stream())
+            if self.ra_ds is not None:
+                call("db2_assemble_matrix", A.pattern.handle, C.byref(self.ra_ds.c_form()),
+                     _coeff_ptr(self.ra_ds), self.prec, _ptr(A.values_tensor()), 1, _stream())
+            if self.rL_ds is not None:
+                call("db2_assemble_vector", A.pattern.handle, C.byref(self.rL_ds.c_form()),
+                     _coeff_ptr(self.rL_ds), _ptr(b.tensor()), 1, _stream())
         return A, b
 
     def _vector_only(self, b):
-        call("db2_assemble_vector", self.rL.V.pattern(False).handle, C.byref(self.rL.c_form()),
+        P = self.rL.V.pattern(False)
+        call("db2_assemble_vector", P.handle, C.byref(self.rL.c_form()),
              _coeff_ptr(self.rL), _ptr(b.tensor()), 0, _stream())
+        if self.rL_ds is not None:
+            call("db2_assemble_vector", P.handle, C.byref(self.rL_ds.c_form()),
+                 _coeff_ptr(self.rL_ds), _ptr(b.tensor()), 1, _stream())
         return b
 
 
@@ -129,6 +181,8 @@ def assemble_system(A_form, b_form, bcs=None, x0=None, form_compiler_parameters=
 
 def assemble_action(a, x, y=None, precision="fp64"):
     """Matrix-free y = A(a) x without forming A (replaces assemble + GenericMatrix::mult)."""
+    if "ds" in a.measures():
+        raise NotImplementedError("matrix-free action of ds terms is not provided")
     rec = recognise(a)
     xt = x.tensor() if hasattr(x, "tensor") else x
     if xt.numel() != rec.V.dim():

@@ -84,6 +84,19 @@ class Mesh(_Handle):
         call("db2_mesh_num_edges", self._h, C.byref(ne))
         return ne.value
 
+    def num_exterior_facets(self):
+        n = C.c_int64()
+        call("db2_mesh_num_exterior_facets", self._h, C.byref(n))
+        return n.value
+
+    def exterior_facets(self):
+        """(cell, local facet) of each exterior facet, in facet-number order."""
+        n = self.num_exterior_facets()
+        cell = np.empty(n, np.uint32)
+        local = np.empty(n, np.int32)
+        call("db2_mesh_exterior_facets", self._h, _ptr(cell), _ptr(local))
+        return cell, local
+
     def coordinates(self):
         x = np.empty((self._nv, self._tdim), np.float64)
         call("db2_mesh_copy", self._h, _ptr(x), None)

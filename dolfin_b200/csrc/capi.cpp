@@ -129,6 +129,27 @@ int db2_mesh_num_edges(db2_mesh m, int64_t* ne) {
   });
 }
 
+int db2_mesh_num_exterior_facets(db2_mesh m, int64_t* n) {
+  return guard([&] {
+    need(m, "mesh");
+    need(n, "n");
+    m->m->compute_exterior_facets();
+    *n = int64_t(m->m->ext_facets.size());
+  });
+}
+
+int db2_mesh_exterior_facets(db2_mesh m, uint32_t* cell, int32_t* local_facet) {
+  return guard([&] {
+    need(m, "mesh");
+    m->m->compute_exterior_facets();
+    const auto& E = m->m->ext_facets;
+    for (size_t i = 0; i < E.size(); ++i) {
+      if (cell) cell[i] = E[i] >> 2;
+      if (local_facet) local_facet[i] = int32_t(E[i] & 3u);
+    }
+  });
+}
+
 int db2_mesh_destroy(db2_mesh m) {
   delete m;
   return DB2_OK;
@@ -242,6 +263,33 @@ int db2_pattern_retile(db2_pattern P, int tile_threads, int seg_cap_bytes) {
   });
 }
 
+int db2_pattern_facet_plan_info(db2_pattern P, int64_t* nbnodes, int64_t* nincidences, int* kf) {
+  return guard([&] {
+    need(P, "pattern");
+    db2::build_facet_plan(*P->P);
+    const db2::FacetPlan& F = *P->P->facets;
+    if (nbnodes) *nbnodes = int64_t(F.bnode.size());
+    if (nincidences) *nincidences = int64_t(F.binc_ptr.back());
+    if (kf) *kf = F.kf;
+  });
+}
+
+int db2_pattern_facet_plan_copy(db2_pattern P, uint32_t* bnode, uint32_t* binc_ptr,
+                                uint32_t* bverts, uint8_t* bslot) {
+  return guard([&] {
+    need(P, "pattern");
+    db2::build_facet_plan(*P->P);
+    const db2::FacetPlan& F = *P->P->facets;
+    auto cp = [](auto* dst, const auto& v) {
+      if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(bnode, F.bnode);
+    cp(binc_ptr, F.binc_ptr);
+    cp(bverts, F.bverts);
+    cp(bslot, F.bslot);
+  });
+}
+
 int db2_pattern_destroy(db2_pattern P) {
   delete P;
   return DB2_OK;
@@ -254,8 +302,11 @@ int db2_assemble_matrix(db2_pattern P, const db2_form* a, const double* w, int p
     need(a, "form");
     need(vals, "vals");
     const db2::FormArgs fa = form_args(a, w);
-    db2::launch_assemble(*P->P, &fa, nullptr, precision, vals, nullptr, add_values != 0, nullptr,
-                         nullptr, stream);
+    if (a->kind == DB2_FORM_FACET_MASS)
+      db2::launch_facet_matrix(*P->P, fa, vals, add_values != 0, nullptr, nullptr, nullptr, stream);
+    else
+      db2::launch_assemble(*P->P, &fa, nullptr, precision, vals, nullptr, add_values != 0, nullptr,
+                           nullptr, stream);
   });
 }
 
@@ -266,8 +317,37 @@ int db2_assemble_vector(db2_pattern P, const db2_form* L, const double* w, doubl
     need(L, "form");
     need(b, "b");
     const db2::FormArgs fl = form_args(L, w);
-    db2::launch_assemble(*P->P, nullptr, &fl, DB2_FP64, nullptr, b, add_values != 0, nullptr,
-                         nullptr, stream);
+    if (L->kind == DB2_FORM_FACET_LOAD)
+      db2::launch_facet_vector(*P->P, fl, b, add_values != 0, nullptr, stream);
+    else
+      db2::launch_assemble(*P->P, nullptr, &fl, DB2_FP64, nullptr, b, add_values != 0, nullptr,
+                           nullptr, stream);
+  });
+}
+
+int db2_assemble_scalar(db2_mesh m, const db2_form* M, const double* w, double* out,
+                        void* stream) {
+  return guard([&] {
+    need(m, "mesh");
+    need(M, "form");
+    need(out, "out");
+    db2::launch_functional(*m->m, form_args(M, w), out, stream);
+  });
+}
+
+int db2_assemble_facets_bc(db2_pattern P, const db2_form* a_ds, const double* wa,
+                           const db2_form* L_ds, const double* wL, const uint8_t* bc_flags,
+                           const double* bc_vals, double* vals, double* b, void* stream) {
+  return guard([&] {
+    need(P, "pattern");
+    need(bc_flags, "bc_flags");
+    need(bc_vals, "bc_vals");
+    need(b, "b");
+    if (a_ds) {
+      need(vals, "vals");
+      db2::launch_facet_matrix(*P->P, form_args(a_ds, wa), vals, true, bc_flags, bc_vals, b, stream);
+    }
+    if (L_ds) db2::launch_facet_vector(*P->P, form_args(L_ds, wL), b, true, bc_flags, stream);
   });
 }
 

@@ -152,6 +152,188 @@ std::shared_ptr<Mesh> make_unit_square(int nx, int ny, int diagonal) {
   return make_mesh(2, nv, x.data(), nc, cells.data());
 }
 
+// Exterior facets: facets (vertex key = the cell's vertices other than local
+// vertex f, sorted) that occur in exactly one cell (Facet::exterior()),
+// listed in key order -- the facet numbering of
+// TopologyComputation::compute_entities_by_key_matching
+// (dolfin/mesh/TopologyComputation.cpp:152-330) restricted to the boundary.
+// Bucketed by the smallest key vertex, sorted by the rest within a bucket.
+void Mesh::compute_exterior_facets() {
+  if (have_facets) return;
+  const int nvc = nverts(tdim), nf = nvc;
+  const int64_t nslots = nc * nf;
+  if (nc >= (int64_t(1) << 30)) fail(DB2_ERR_UNSUPPORTED, "too many cells for facet records");
+  std::vector<uint32_t> start(nv + 1, 0);
+  auto key_of = [&](int64_t c, int f, uint32_t k[3]) {
+    int m = 0;
+    for (int a = 0; a < nvc; ++a)
+      if (a != f) k[m++] = cells[c * nvc + a];  // cell vertices are sorted
+    if (m < 3) k[2] = 0;
+  };
+  for (int64_t c = 0; c < nc; ++c)
+    for (int f = 0; f < nf; ++f) {
+      uint32_t k[3];
+      key_of(c, f, k);
+      start[k[0] + 1]++;
+    }
+  for (int64_t v = 0; v < nv; ++v) start[v + 1] += start[v];
+  struct Entry { uint64_t rest; uint32_t slot; };
+  std::vector<Entry> bucket(nslots);
+  std::vector<uint32_t> fillp(start.begin(), start.end() - 1);
+  for (int64_t c = 0; c < nc; ++c)
+    for (int f = 0; f < nf; ++f) {
+      uint32_t k[3];
+      key_of(c, f, k);
+      const uint64_t rest = tdim == 3 ? (uint64_t(k[1]) << 32) | k[2] : uint64_t(k[1]);
+      bucket[fillp[k[0]]++] = Entry{rest, uint32_t(c << 2 | f)};
+    }
+  std::vector<uint32_t> count(nv + 1, 0);
+  parallel_for(nv, [&](int64_t b, int64_t e) {
+    for (int64_t v = b; v < e; ++v) {
+      Entry* lo = bucket.data() + start[v];
+      Entry* hi = bucket.data() + start[v + 1];
+      std::sort(lo, hi, [](const Entry& x, const Entry& y) {
+        return x.rest < y.rest || (x.rest == y.rest && x.slot < y.slot);
+      });
+      uint32_t u = 0;
+      for (Entry* it = lo; it != hi;) {
+        Entry* j = it + 1;
+        while (j != hi && j->rest == it->rest) ++j;
+        if (j - it == 1) ++u;
+        it = j;
+      }
+      count[v + 1] = u;
+    }
+  });
+  for (int64_t v = 0; v < nv; ++v) count[v + 1] += count[v];
+  ext_facets.assign(count[nv], 0);
+  parallel_for(nv, [&](int64_t b, int64_t e) {
+    for (int64_t v = b; v < e; ++v) {
+      uint32_t o = count[v];
+      Entry* lo = bucket.data() + start[v];
+      Entry* hi = bucket.data() + start[v + 1];
+      for (Entry* it = lo; it != hi;) {
+        Entry* j = it + 1;
+        while (j != hi && j->rest == it->rest) ++j;
+        if (j - it == 1) ext_facets[o++] = it->slot;
+        it = j;
+      }
+    }
+  });
+  have_facets = true;
+}
+
+// Exterior-facet plan (see FacetPlan).  Facet nodes in canonical facet order:
+// the facet's vertices (ascending local index), then for P2 its edges in the
+// local edge order of a triangle ((1,2), (0,2), (0,1)) or the one edge of an
+// interval, in facet-local vertex indices.
+void build_facet_plan(Pattern& P) {
+  if (P.facets) return;
+  const Space& V = *P.V;
+  Mesh& m = *V.mesh;
+  m.compute_exterior_facets();
+  const int D = m.tdim, nvc = nverts(D), k = V.k;
+  const int nfe = V.degree == 2 ? (D == 3 ? 3 : 1) : 0;
+  const int kf = D + nfe;
+  static const int kFE3[3][2] = {{1, 2}, {0, 2}, {0, 1}};
+  static const int kFE2[1][2] = {{0, 1}};
+  const int (*FE)[2] = D == 3 ? kFE3 : kFE2;
+  const int (*CE)[2] = etab(D);
+  auto cell_edge = [&](int a, int b) {
+    for (int e = 0; e < nedges(D); ++e)
+      if ((CE[e][0] == a && CE[e][1] == b) || (CE[e][0] == b && CE[e][1] == a)) return e;
+    return -1;
+  };
+  auto facet_edge = [&](int p, int q) {
+    for (int e = 0; e < nfe; ++e)
+      if ((FE[e][0] == p && FE[e][1] == q) || (FE[e][0] == q && FE[e][1] == p)) return e;
+    return -1;
+  };
+  const int64_t nfac = int64_t(m.ext_facets.size());
+  // facet nodes (global) and facet vertex ids of every exterior facet
+  std::vector<uint32_t> fnode(size_t(nfac) * kf), fvert(size_t(nfac) * D);
+  for (int64_t i = 0; i < nfac; ++i) {
+    const uint32_t c = m.ext_facets[i] >> 2, fl = m.ext_facets[i] & 3u;
+    int av[3], mm = 0;
+    for (int a = 0; a < nvc; ++a)
+      if (a != int(fl)) av[mm++] = a;
+    for (int t = 0; t < D; ++t) {
+      fnode[i * kf + t] = V.cell_nodes[int64_t(c) * k + av[t]];
+      fvert[i * D + t] = m.cells[int64_t(c) * nvc + av[t]];
+    }
+    for (int e = 0; e < nfe; ++e)
+      fnode[i * kf + D + e] = V.cell_nodes[int64_t(c) * k + nvc + cell_edge(av[FE[e][0]], av[FE[e][1]])];
+  }
+  auto F = std::make_unique<FacetPlan>();
+  F->kf = kf;
+  // incidences grouped by node, in facet order within a node
+  std::vector<uint32_t> cnt(V.nnodes + 1, 0);
+  for (uint32_t n : fnode) cnt[n + 1]++;
+  for (int64_t n = 0; n < V.nnodes; ++n) cnt[n + 1] += cnt[n];
+  std::vector<uint32_t> order(fnode.size());
+  {
+    std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
+    for (size_t s = 0; s < fnode.size(); ++s) order[fill[fnode[s]]++] = uint32_t(s);
+  }
+  F->binc_ptr.push_back(0);
+  for (int64_t n = 0; n < V.nnodes; ++n)
+    if (cnt[n + 1] > cnt[n]) {
+      F->bnode.push_back(uint32_t(n));
+      F->binc_ptr.push_back(cnt[n + 1]);
+    }
+  const size_t ninc = order.size();
+  F->bverts.resize(ninc * D);
+  F->bslot.assign(ninc * 8, 0);
+  for (size_t s = 0; s < ninc; ++s) {
+    const uint32_t e = order[s];
+    const int64_t i = e / kf;
+    const int t = int(e % kf);
+    const uint32_t node = fnode[e];
+    // relabelled facet vertex order: row vertex first, or row edge's two ends
+    int ord[3], mm = 0;
+    bool used[3] = {false, false, false};
+    auto put = [&](int a) {
+      ord[mm++] = a;
+      used[a] = true;
+    };
+    if (t < D) {
+      put(t);
+    } else {
+      put(FE[t - D][0]);
+      put(FE[t - D][1]);
+    }
+    for (int a = 0; a < D; ++a)
+      if (!used[a]) put(a);
+    for (int a = 0; a < D; ++a) F->bverts[s * D + a] = fvert[i * D + ord[a]];
+    // column slots of the relabelled facet nodes within the row of `node`
+    const int32_t* rb = P.node_cols.data() + P.node_rowptr[node];
+    const int32_t* re = P.node_cols.data() + P.node_rowptr[node + 1];
+    for (int j = 0; j < kf; ++j) {
+      int src = j < D ? ord[j] : D + facet_edge(ord[FE[j - D][0]], ord[FE[j - D][1]]);
+      const uint32_t col = fnode[i * kf + src];
+      const int32_t* it = std::lower_bound(rb, re, int32_t(col));
+      if (it == re || *it != int32_t(col)) fail(DB2_ERR_INDEX, "facet node missing from the pattern");
+      F->bslot[s * 8 + j] = uint8_t(it - rb);
+    }
+  }
+  P.facets = std::move(F);
+}
+
+const FacetPlan& Pattern::facet_plan() {
+  if (!facets || !facets->d_binc_ptr.ptr) {
+    build_facet_plan(*this);
+    FacetPlan& F = *facets;
+    auto up = [](DeviceBuffer& d, const auto& v) {
+      if (!v.empty()) d.upload(v.data(), v.size() * sizeof(v[0]));
+    };
+    up(F.d_bnode, F.bnode);
+    up(F.d_binc_ptr, F.binc_ptr);
+    up(F.d_bverts, F.bverts);
+    up(F.d_bslot, F.bslot);
+  }
+  return *facets;
+}
+
 // Entity numbering of edges: equivalent to sorting all (cell, local edge)
 // entries by their sorted vertex key and numbering distinct keys in order
 // (TopologyComputation::compute_entities_by_key_matching,

@@ -41,12 +41,19 @@ struct Mesh {
   int64_t ne = 0;
   std::vector<uint32_t> cell_edges;  // nc * nedges(tdim), UFC local edge order
   std::vector<uint32_t> edge_vertices;  // ne * 2, sorted vertex pair of each edge
-  // device copies: coordinates padded to 4 (3D) or 2 (2D) doubles per vertex
-  DeviceBuffer d_x, d_cells;
+  // exterior facets (computed on demand), in facet-number order -- sorted
+  // vertex key, as TopologyComputation numbers entities: cell << 2 | local
+  // facet (facet i of a simplex is opposite its local vertex i)
+  bool have_facets = false;
+  std::vector<uint32_t> ext_facets;
+  // device copies: 4 doubles per vertex (coordinates, then the per-call
+  // coefficient values the assembly kernels read with the coordinates)
+  DeviceBuffer d_x, d_cells, d_ext_facets, d_partials;
   bool on_device = false;
   void ensure_device();      // first GPU use: upload coordinates and cells
   void upload_coordinates();
   void compute_edges();
+  void compute_exterior_facets();
 };
 
 int nverts(int tdim);
@@ -74,6 +81,21 @@ struct Tile {
   int32_t comp;   // test component c of the tile's rows
   int32_t n0, n1; // node range [n0, n1)
   int32_t pad;
+};
+
+// Exterior-facet plan of a pattern: each boundary node (row owner) with its
+// incidences (exterior facet, facet node) in facet-number order -- the order
+// of Assembler::assemble_exterior_facets' facet loop.  Each incidence holds
+// the facet's vertex ids relabelled so that the row node is canonical (facet
+// vertex 0, or facet edge (0,1)), and the column slots within the node row of
+// the facet's nodes in canonical facet order.
+struct FacetPlan {
+  int kf = 0;                        // nodes per facet
+  std::vector<uint32_t> bnode;       // boundary nodes, ascending
+  std::vector<uint32_t> binc_ptr;    // bnode.size() + 1
+  std::vector<uint32_t> bverts;      // tdim vertex ids per incidence
+  std::vector<uint8_t> bslot;        // 8 slots per incidence (kf used)
+  DeviceBuffer d_bnode, d_binc_ptr, d_bverts, d_bslot;
 };
 
 struct Pattern {
@@ -108,6 +130,8 @@ struct Pattern {
   void ensure_device();      // first GPU use: upload the plan, expand the CSR
   // dof-level CSR on the host (component expansion of the node graph)
   void csr_host(int32_t* rowptr, int32_t* cols) const;
+  std::unique_ptr<FacetPlan> facets;
+  const FacetPlan& facet_plan();     // built and uploaded on first use
 };
 
 // Relabelling of a cell so that local node `li` becomes canonical: for a
@@ -124,6 +148,9 @@ std::shared_ptr<Mesh> make_mesh(int tdim, int64_t nv, const double* x, int64_t n
 std::shared_ptr<Space> make_space(std::shared_ptr<Mesh> m, int degree, int vsize);
 std::shared_ptr<Pattern> make_pattern(std::shared_ptr<Space> V, bool keep_diagonal,
                                       int tile_threads = 0, int seg_cap_bytes = 0);
+// Host-side facet plan of a pattern (no device work); Pattern::facet_plan()
+// also uploads it.
+void build_facet_plan(Pattern& P);
 // Re-cut the tiles of an existing plan (autotuning), re-uploading d_tiles.
 void retile(Pattern& P, int tile_threads, int seg_cap_bytes);
 // Tiles of a pattern for a launch shape (pure; does not modify P).
@@ -137,6 +164,12 @@ struct FormArgs {
 void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int precision,
                      double* vals, double* b, bool add_values, const uint8_t* bc_flags,
                      const double* bc_vals, void* stream);
+// Exterior-facet and functional assembly (facets.cu).
+void launch_facet_matrix(Pattern& P, const FormArgs& a, double* vals, bool add_values,
+                         const uint8_t* bc_flags, const double* bc_vals, double* b, void* stream);
+void launch_facet_vector(Pattern& P, const FormArgs& L, double* b, bool add_values,
+                         const uint8_t* bc_flags, void* stream);
+void launch_functional(Mesh& m, const FormArgs& M, double* out, void* stream);
 void launch_apply(const Pattern& P, const FormArgs& a, int precision, const double* x, double* y,
                   void* stream);
 void launch_vjp(const Pattern& P, const FormArgs& a, const FormArgs& L, int precision,

@@ -10,8 +10,13 @@ arguments' values and gradients, and identified as one of the named forms:
     kappa * inner(grad(u), grad(v)) * dx     kappa: 1, Constant, P1 Function, c*Function
     inner(sigma(u), epsilon(v)) * dx          2 mu eps:eps + lmbda div div  (mu, lmbda fitted)
     f * v * dx, inner(f, v) * dx             f: Constant (vector), P1 Function, c*Function
+    w * u * v * ds                            boundary mass (Robin), w as kappa (scalar spaces)
+    g * v * ds, inner(t, v) * ds              Neumann load, g as f; t a constant vector
+    w * dx, w * ds                            functionals: w = Constant, P1 Function, c*x[i]
 
-Anything else raises NotImplementedError: no other kernels exist.
+A form may hold dx and ds terms (cell part + exterior-facet part, assembled
+as the reference's cell loop followed by its exterior-facet loop).  Anything
+else raises NotImplementedError: no other kernels exist.
 """
 from __future__ import annotations
 
@@ -243,28 +248,67 @@ class Indexed(Expr):
         return self.ops[0].ev(env)[:, self.i]
 
 
-class Measure:
-    def __init__(self, name="dx"):
-        self.name = name
+class SpatialCoordinate(Expr):
+    """x = SpatialCoordinate(mesh); x[i] is the i-th coordinate (P1 on affine cells)."""
 
-    def __call__(self, *a, **k):
-        if a or k.get("subdomain_data") is not None or k.get("subdomain_id") is not None:
+    def __init__(self, mesh):
+        self.mesh, self.ops = mesh, ()
+        self.shape = (mesh.geometry_dim(),)
+
+    def ev(self, env):
+        return env["x"]
+
+
+class Measure:
+    """dx (cells) or ds (exterior facets), optionally bound to a mesh: dx(mesh)."""
+
+    def __init__(self, name="dx", domain=None):
+        self.name, self.domain = name, domain
+
+    def __call__(self, *a, domain=None, subdomain_data=None, subdomain_id=None, **k):
+        if a and hasattr(a[0], "geometry_dim"):
+            domain, a = a[0], a[1:]
+        if a or k or subdomain_data is not None or subdomain_id is not None:
             raise NotImplementedError("subdomain integrals are not provided")
-        return self
+        return Measure(self.name, domain if domain is not None else self.domain)
 
     def __rmul__(self, integrand):
         return Form([(as_expr(integrand), self)])
 
 
 dx = Measure("dx")
+ds = Measure("ds")
 
 
 class Form:
     def __init__(self, terms):
         for _, m in terms:
-            if m.name != "dx":
-                raise NotImplementedError(f"only cell integrals (dx) are provided, got {m.name}")
+            if m.name not in ("dx", "ds"):
+                raise NotImplementedError(
+                    f"cell (dx) and exterior facet (ds) integrals are provided, got {m.name}")
         self.terms = list(terms)
+
+    def part(self, name):
+        """The terms integrated over measure `name` ("dx" or "ds"), or None."""
+        t = [(e, m) for e, m in self.terms if m.name == name]
+        return Form(t) if t else None
+
+    def measures(self):
+        return sorted({m.name for _, m in self.terms})
+
+    def domain(self):
+        """The mesh of the form: from its measures, arguments or coefficients."""
+        for _, m in self.terms:
+            if m.domain is not None:
+                return m.domain
+        for n in self.integrand().walk():
+            if isinstance(n, Argument):
+                return n.V.mesh()
+            if isinstance(n, SpatialCoordinate):
+                return n.mesh
+            if hasattr(n, "function_space"):
+                return n.function_space().mesh()
+        return None
 
     def __add__(self, o):
         return Form(self.terms + o.terms)
@@ -328,6 +372,8 @@ class Recognised:
 
 def _env(rng, args, fvals=None, zero_values=False, zero_grads=False):
     env = {"val": {}, "grad": {}, "f": fvals or {}}
+    for V in args.values():
+        env["x"] = rng.standard_normal((_NPROBE, V.mesh().geometry_dim()))
     for num, V in args.items():
         vs, d = V.value_size(), V.mesh().geometry_dim()
         vshape = (_NPROBE,) if vs == 1 else (_NPROBE, vs)
@@ -341,10 +387,132 @@ def _close(a, b, tol=1e-10):
     return np.allclose(a, b, rtol=tol, atol=tol * (1.0 + np.max(np.abs(b))))
 
 
-def recognise(form):
+def recognise_parts(form):
+    """(cell part, exterior-facet part) of a rank 1/2 form, each a Recognised
+    or None."""
+    if not isinstance(form, Form):
+        raise TypeError("expected a Form")
+    fx, fs = form.part("dx"), form.part("ds")
+    cell = recognise(fx) if fx is not None else None
+    facet = recognise_facet(fs) if fs is not None else None
+    if cell is not None and facet is not None and cell.V is not facet.V:
+        raise ValueError("dx and ds terms on different spaces")
+    return cell, facet
+
+
+def recognise_facet(form):
+    """Exterior-facet part: w*u*v*ds, g*v*ds or inner(t, v)*ds."""
+    from . import _capi
+    args = form.arguments()
+    rank = len(args)
+    fs, _ = form.coefficients()
+    if len(fs) > 1:
+        raise NotImplementedError("ds forms with more than one Function coefficient are not provided")
+    func = fs[0] if fs else None
+    if func is not None and (func.function_space().degree() != 1 or func.function_space().value_size() != 1):
+        raise NotImplementedError("coefficients must be scalar P1 Functions")
+    rng = np.random.default_rng(20190402)
+    I = form.integrand()
+
+    def ev(env):
+        return I.ev(env)
+
+    def fvals(v):
+        return {func: np.full(_NPROBE, v)} if func is not None else {}
+
+    if rank == 2:
+        V = args[0]
+        if args[1] is not V:
+            raise NotImplementedError("rectangular (V x W) forms are not provided")
+        if V.value_size() != 1:
+            raise NotImplementedError("boundary mass on vector spaces is not provided")
+        env = _env(rng, args, fvals(1.0))
+        full = ev(env)
+        env0 = dict(env, grad={k: np.zeros_like(v) for k, v in env["grad"].items()})
+        if not _close(ev(env0), full):
+            raise NotImplementedError("only w*u*v*ds bilinear facet forms are provided")
+        uv = env["val"][0] * env["val"][1]
+        A1 = full / uv
+        if not np.allclose(A1, A1[0], rtol=1e-10):
+            raise NotImplementedError("bilinear facet form is not w*u*v*ds")
+        alpha = _unit_probe(ev, args, fvals(1.0), grads=False)
+        if func is None:
+            coeff = _capi.COEFF_NONE if alpha == 1.0 else _capi.COEFF_CONSTANT
+            return Recognised(_capi.FORM_FACET_MASS, V, coeff, None, (alpha, 0, 0))
+        A2 = ev(dict(env, f=fvals(2.0))) / uv
+        if not _close(A2, 2.0 * A1):
+            raise NotImplementedError("coefficient must enter linearly as a factor")
+        coeff = _capi.COEFF_P1 if alpha == 1.0 else _capi.COEFF_P1_SCALED
+        return Recognised(_capi.FORM_FACET_MASS, V, coeff, func, (alpha, 0, 0))
+    if rank == 1:
+        # the linear recogniser, with the facet kind
+        r = recognise(form, _kind=_capi.FORM_FACET_LOAD)
+        return r
+    raise NotImplementedError("use assemble() for functionals")
+
+
+def recognise_functional(form):
+    """Rank-0 form: [(kind, mesh, coeff, function, constant)] for its dx / ds
+    parts; integrands c, c*f (P1 Function f) or c*x[i]."""
+    from . import _capi
+    from .function import Function
+    if form.rank() != 0:
+        raise ValueError("not a functional")
+    out = []
+    for name, kind in (("dx", _capi.FORM_FUNCTIONAL), ("ds", _capi.FORM_FACET_FUNCTIONAL)):
+        part = form.part(name)
+        if part is None:
+            continue
+        mesh = part.domain() or form.domain()
+        if mesh is None:
+            raise ValueError("functional without a mesh: integrate over dx(mesh) / ds(mesh)")
+        I = part.integrand()
+        fs = [n for n in I.walk() if isinstance(n, Function)]
+        xs = [n for n in I.walk() if isinstance(n, SpatialCoordinate)]
+        if len(set(map(id, fs))) > 1 or (fs and xs):
+            raise NotImplementedError("functionals of one P1 Function or one coordinate are provided")
+        rng = np.random.default_rng(20190403)
+        gd = mesh.geometry_dim()
+        env = {"val": {}, "grad": {}, "f": {}, "x": rng.standard_normal((_NPROBE, gd))}
+        if fs:
+            f = fs[0]
+            if f.function_space().degree() != 1 or f.function_space().value_size() != 1:
+                raise NotImplementedError("functional coefficients must be scalar P1 Functions")
+            v1 = I.ev(dict(env, f={f: np.ones(_NPROBE)}))
+            v2 = I.ev(dict(env, f={f: np.full(_NPROBE, 2.0)}))
+            if not (np.allclose(v1, v1[0], rtol=1e-12) and _close(v2, 2.0 * v1)):
+                raise NotImplementedError("functional must be c * f for a P1 Function f")
+            alpha = float(v1[0])
+            coeff = _capi.COEFF_P1 if alpha == 1.0 else _capi.COEFF_P1_SCALED
+            out.append((kind, mesh, coeff, f, (alpha, 0.0, 0.0)))
+        elif xs:
+            full = I.ev(env)
+            alphas = []
+            for i in range(gd):
+                e = np.zeros((_NPROBE, gd))
+                e[:, i] = 1.0
+                alphas.append(float(I.ev(dict(env, x=e))[0]))
+            if not _close(env["x"] @ np.array(alphas), full) or sum(a != 0.0 for a in alphas) != 1:
+                raise NotImplementedError("functional must be c * x[i]")
+            i = next(k for k, a in enumerate(alphas) if a != 0.0)
+            out.append((kind, mesh, _capi.COEFF_COORD, None, (alphas[i], float(i), 0.0)))
+        else:
+            v = I.ev(env)
+            if not np.allclose(v, v[0], rtol=1e-12):
+                raise NotImplementedError("functional integrand is not constant")
+            out.append((kind, mesh, _capi.COEFF_CONSTANT, None, (float(v[0]), 0.0, 0.0)))
+    return out
+
+
+def recognise(form, _kind=None):
+    """Cell (dx) part of a rank 1/2 form: one of the engine's cell kernels."""
     from . import _capi
     if not isinstance(form, Form):
         raise TypeError("expected a Form")
+    if _kind is None and "ds" in form.measures():
+        if "dx" not in form.measures():
+            raise NotImplementedError("the form has only ds terms: use recognise_parts")
+        form = form.part("dx")
     args = form.arguments()
     rank = len(args)
     fs, _ = form.coefficients()
@@ -407,6 +575,7 @@ def recognise(form):
         return Recognised(_capi.FORM_ELASTICITY, V, _capi.COEFF_NONE, None, (0, 0, 0), mu, lmbda)
 
     if rank == 1:
+        lkind = _kind if _kind is not None else _capi.FORM_LOAD
         V = args[0]
         env = _env(rng, args, fvals(1.0))
         full = ev(env)
@@ -419,12 +588,12 @@ def recognise(form):
                 raise NotImplementedError("linear form is not f*v*dx")
             alpha = _unit_probe(ev, args, fvals(1.0), grads=False)
             if func is None:
-                return Recognised(_capi.FORM_LOAD, V, _capi.COEFF_CONSTANT, None, (alpha, 0, 0))
+                return Recognised(lkind, V, _capi.COEFF_CONSTANT, None, (alpha, 0, 0))
             F2 = ev(dict(env, f=fvals(2.0))) / env["val"][0]
             if not _close(F2, 2.0 * F1):
                 raise NotImplementedError("load coefficient must enter linearly")
             coeff = _capi.COEFF_P1 if alpha == 1.0 else _capi.COEFF_P1_SCALED
-            return Recognised(_capi.FORM_LOAD, V, coeff, func, (alpha, 0, 0))
+            return Recognised(lkind, V, coeff, func, (alpha, 0, 0))
         if func is not None:
             raise NotImplementedError("vector loads take a Constant")
         vs = V.value_size()
@@ -435,9 +604,9 @@ def recognise(form):
         chk = np.einsum("pi,i->p", env["val"][0], np.array(fvec))
         if not _close(chk, full):
             raise NotImplementedError("vector load is not inner(f, v) with constant f")
-        return Recognised(_capi.FORM_LOAD, V, _capi.COEFF_CONSTANT, None, tuple(fvec) + (0.0,) * (3 - vs))
+        return Recognised(lkind, V, _capi.COEFF_CONSTANT, None, tuple(fvec) + (0.0,) * (3 - vs))
 
-    raise NotImplementedError("functionals (rank-0 forms) are not provided by the engine")
+    raise NotImplementedError("functionals: use assemble() (rank-0 forms)")
 
 
 def _unit_probe(ev, args, fv, grads):

@@ -51,14 +51,23 @@ typedef struct db2_batch_t* db2_batch;
 enum db2_form_kind {
   DB2_FORM_DIFFUSION = 1,  /* a = kappa*inner(grad(u), grad(v))*dx          */
   DB2_FORM_LOAD = 2,       /* L = f*v*dx (scalar), inner(f, v)*dx (vector)  */
-  DB2_FORM_ELASTICITY = 3  /* a = inner(sigma(u), epsilon(v))*dx,
+  DB2_FORM_ELASTICITY = 3, /* a = inner(sigma(u), epsilon(v))*dx,
                               sigma = 2 mu epsilon + lmbda tr(epsilon) I    */
+  /* exterior facet integrals (Assembler::assemble_exterior_facets,
+     dolfin/fem/Assembler.cpp:196-288) and functionals                      */
+  DB2_FORM_FACET_MASS = 4, /* a = w*u*v*ds (scalar spaces)                  */
+  DB2_FORM_FACET_LOAD = 5, /* L = w*v*ds (scalar), inner(t, v)*ds (vector,
+                              t = constant[0..2])                           */
+  DB2_FORM_FUNCTIONAL = 6, /* M = w*dx                                      */
+  DB2_FORM_FACET_FUNCTIONAL = 7 /* M = w*ds                                 */
 };
 enum db2_coeff_kind {
   DB2_COEFF_NONE = 0,      /* coefficient 1                                 */
   DB2_COEFF_CONSTANT = 1,  /* dolfin Constant: constant[] (scalar or vector)*/
   DB2_COEFF_P1 = 2,        /* P1 Function: device array of vertex values     */
-  DB2_COEFF_P1_SCALED = 3  /* constant[0] * P1 Function                      */
+  DB2_COEFF_P1_SCALED = 3, /* constant[0] * P1 Function                      */
+  DB2_COEFF_COORD = 4      /* constant[0] * x[i], i = (int)constant[1]
+                              (SpatialCoordinate; functionals only)         */
 };
 enum db2_precision {
   DB2_FP64 = 0,            /* geometry, contraction, accumulation in FP64    */
@@ -99,6 +108,12 @@ int db2_mesh_copy(db2_mesh m, double* coords, uint32_t* cells);
 int db2_mesh_set_coordinates(db2_mesh m, const double* coords);
 /* Number of edges (mesh.init(1); TopologyComputation key matching). */
 int db2_mesh_num_edges(db2_mesh m, int64_t* ne);
+/* Exterior facets (Facet::exterior(): one incident cell), in facet-number
+   order (sorted vertex key, TopologyComputation key matching): count, and
+   host copies of each facet's cell and local facet index (facet i of a
+   simplex is opposite local vertex i). */
+int db2_mesh_num_exterior_facets(db2_mesh m, int64_t* n);
+int db2_mesh_exterior_facets(db2_mesh m, uint32_t* cell, int32_t* local_facet);
 int db2_mesh_destroy(db2_mesh m);
 
 /* ---- function space + dofmap (DofMap, DofMapBuilder::build) ----------- */
@@ -131,6 +146,15 @@ int db2_pattern_plan_info(db2_pattern P, int64_t* nnodes, int64_t* nincidences, 
                           int64_t* ntiles, int64_t* ngroups, int64_t* ntypes);
 int db2_pattern_plan_copy(db2_pattern P, int32_t* node_rowptr, int32_t* node_cols,
                           uint32_t* inc_ptr, uint32_t* inc, uint8_t* pos, int32_t* tiles);
+/* Diagnostics of the exterior-facet plan (no reference counterpart; used by
+   the tests): boundary nodes, their (exterior facet, facet node) incidences
+   in facet-number order (binc_ptr[nbnodes+1]), per incidence the facet's
+   tdim vertex ids relabelled so the row node is canonical (bverts) and the
+   CSR column slots of its kf facet nodes within the node's row (bslot, 8
+   bytes per incidence). */
+int db2_pattern_facet_plan_info(db2_pattern P, int64_t* nbnodes, int64_t* nincidences, int* kf);
+int db2_pattern_facet_plan_copy(db2_pattern P, uint32_t* bnode, uint32_t* binc_ptr,
+                                uint32_t* bverts, uint8_t* bslot);
 /* Re-cut the pattern's tiles (launch shape of the assembly kernel): CTAs of
    tile_threads threads, row segments of at most seg_cap_bytes of shared
    memory.  Results do not depend on the launch shape (bitwise). */
@@ -146,6 +170,19 @@ int db2_assemble_matrix(db2_pattern P, const db2_form* a, const double* w, int p
 /* Assembler::assemble(b, L) for a linear form: b[N] (device). */
 int db2_assemble_vector(db2_pattern P, const db2_form* L, const double* w, double* b,
                         int add_values, void* stream);
+/* db2_assemble_matrix / db2_assemble_vector also take DB2_FORM_FACET_MASS /
+   DB2_FORM_FACET_LOAD: the exterior-facet loop of Assembler::assemble
+   (Assembler.cpp:196-288).  A form with dx and ds terms is assembled by the
+   cell call, then the facet call with add_values = 1 (the reference's cell
+   loop, then facet loop). */
+
+/* double assemble(const Form&) (dolfin/fem/assemble.h:66) for
+   M = w*dx (DB2_FORM_FUNCTIONAL) or w*ds (DB2_FORM_FACET_FUNCTIONAL), w =
+   1, Constant, P1 Function (w: device vertex values) or x[i]
+   (DB2_COEFF_COORD): writes the value to out[0] (device).  Deterministic:
+   a fixed-order reduction. */
+int db2_assemble_scalar(db2_mesh m, const db2_form* M, const double* w, double* out,
+                        void* stream);
 /* SystemAssembler(a, L).assemble(A, b) (dolfin/fem/SystemAssembler.cpp:138-301,
    cell_wise_assembly :303-492) without boundary conditions: A and b in one
    pass sharing the geometry of each cell. */
@@ -158,6 +195,14 @@ int db2_assemble_system(db2_pattern P, const db2_form* a, const double* wa, cons
 int db2_assemble_system_bc(db2_pattern P, const db2_form* a, const double* wa, const db2_form* L,
                            const double* wL, const uint8_t* bc_flags, const double* bc_vals,
                            int precision, double* vals, double* b, void* stream);
+/* The exterior-facet terms of a SystemAssembler pass with DirichletBC
+   (SystemAssembler.cpp:417-470 adds them to the cell tensor before
+   apply_bc): call after db2_assemble_system_bc with the same bc_flags /
+   bc_vals.  a_ds (DB2_FORM_FACET_MASS) or L_ds (DB2_FORM_FACET_LOAD) may be
+   NULL; Dirichlet rows take nothing, Dirichlet columns move to b. */
+int db2_assemble_facets_bc(db2_pattern P, const db2_form* a_ds, const double* wa,
+                           const db2_form* L_ds, const double* wL, const uint8_t* bc_flags,
+                           const double* bc_vals, double* vals, double* b, void* stream);
 /* Matrix-free action y = A(a) x (device x[N], y[N]); replaces assembling A
    and calling GenericMatrix::mult (dolfin/la/GenericMatrix.h). */
 int db2_apply(db2_pattern P, const db2_form* a, const double* w, int precision, const double* x,

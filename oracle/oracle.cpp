@@ -440,6 +440,21 @@ struct FacetTabulator {
         for (int a = 0; a <= d; ++a) lam[fl][p * (d + 1) + a] = l[a];
         if (k0) eval_basis(f.family0, f.degree0, d, X, &phi0[fl][p * k0], dummy.data());
         if (k1) eval_basis(f.family1, f.degree1, d, X, &phi1[fl][p * k1], dummy.data());
+        // basis functions of nodes off the facet (its opposite vertex, and for
+        // P2 the edges through that vertex) vanish identically on it: store
+        // exact zeros rather than the roundoff of lambda_0 = 1 - sum X
+        for (int i = 0; i < std::max(k0, k1); ++i) {
+          bool on = true;
+          if (i <= d) on = i != fl;
+          else {
+            const int (*E)[2] = edge_table(d);
+            on = E[i - d - 1][0] != fl && E[i - d - 1][1] != fl;
+          }
+          if (!on) {
+            if (i < k0) phi0[fl][p * k0 + i] = 0.0;
+            if (i < k1) phi1[fl][p * k1 + i] = 0.0;
+          }
+        }
       }
     }
   }

@@ -142,3 +142,90 @@ def test_recogniser_identifies_named_forms():
     assert r.kind == _capi.FORM_LOAD and r.constant == (0.0, 0.0, -1.0)
     with pytest.raises(NotImplementedError):
         recognise(u[0] * v[0] * d2.dx)
+
+
+@pytest.mark.parametrize("tdim,n", [(2, 6), (3, 3)])
+def test_exterior_facets_match_oracle(orc, tdim, n):
+    # facet-number (sorted key) order, cell and local facet of each
+    m = d2.UnitSquareMesh(n, n) if tdim == 2 else d2.UnitCubeMesh(n, n, n)
+    om = orc.unit_square_mesh(n, n) if tdim == 2 else orc.unit_cube_mesh(n, n, n)
+    cell, local = m.exterior_facets()
+    oc, ol = orc.exterior_facets(om)
+    assert np.array_equal(cell, oc) and np.array_equal(local, ol)
+
+
+def test_recogniser_facet_and_functional_parts():
+    from dolfin_b200.ufl import recognise_functional, recognise_parts
+    m = d2.UnitCubeMesh(1, 1, 1)
+    V = d2.FunctionSpace(m, "Lagrange", 2)
+    W = d2.FunctionSpace(m, "Lagrange", 1)
+    u, v = d2.TrialFunction(V), d2.TestFunction(V)
+    g = d2.Function(W)
+    cell, facet = recognise_parts(d2.inner(d2.grad(u), d2.grad(v)) * d2.dx + 2.5 * g * u * v * d2.ds)
+    assert cell.kind == _capi.FORM_DIFFUSION
+    assert facet.kind == _capi.FORM_FACET_MASS and facet.coeff == _capi.COEFF_P1_SCALED
+    assert facet.constant[0] == 2.5 and facet.function is g
+    cell, facet = recognise_parts(g * v * d2.ds)
+    assert cell is None and facet.kind == _capi.FORM_FACET_LOAD and facet.coeff == _capi.COEFF_P1
+    VV = d2.VectorFunctionSpace(m, "Lagrange", 1)
+    cell, facet = recognise_parts(d2.inner(d2.Constant((1.0, 0.0, -2.0)), d2.TestFunction(VV)) * d2.ds)
+    assert facet.kind == _capi.FORM_FACET_LOAD and facet.constant == (1.0, 0.0, -2.0)
+    x = d2.SpatialCoordinate(m)
+    parts = recognise_functional(3.0 * x[2] * d2.dx(m) + d2.Constant(1.0) * d2.ds(m))
+    assert parts[0][0] == _capi.FORM_FUNCTIONAL and parts[0][2] == _capi.COEFF_COORD
+    assert parts[0][4][:2] == (3.0, 2.0)
+    assert parts[1][0] == _capi.FORM_FACET_FUNCTIONAL and parts[1][4][0] == 1.0
+    with pytest.raises(NotImplementedError):
+        recognise_parts(d2.inner(d2.grad(u), d2.grad(v)) * d2.ds)
+    with pytest.raises(NotImplementedError):
+        d2.Constant(1.0) * d2.ds(m, subdomain_id=1)
+
+
+@pytest.mark.parametrize("tdim,deg", [(2, 1), (2, 2), (3, 1), (3, 2)])
+def test_facet_plan_slots_point_at_the_facet_nodes(orc, tdim, deg):
+    import ctypes as C
+    n = 3
+    m = d2.UnitSquareMesh(n, n) if tdim == 2 else d2.UnitCubeMesh(n, n, n)
+    om = orc.unit_square_mesh(n, n) if tdim == 2 else orc.unit_cube_mesh(n, n, n)
+    V = d2.FunctionSpace(m, "Lagrange", deg)
+    P = V.pattern()
+    nb, ni, kf = C.c_int64(), C.c_int64(), C.c_int()
+    _capi.call("db2_pattern_facet_plan_info", P.handle, C.byref(nb), C.byref(ni), C.byref(kf))
+    bnode = np.empty(nb.value, np.uint32)
+    bptr = np.empty(nb.value + 1, np.uint32)
+    bverts = np.empty(ni.value * tdim, np.uint32)
+    bslot = np.empty(ni.value * 8, np.uint8)
+    ptr = lambda a: C.c_void_p(a.ctypes.data)
+    _capi.call("db2_pattern_facet_plan_copy", P.handle, ptr(bnode), ptr(bptr), ptr(bverts), ptr(bslot))
+    bverts, bslot, kf = bverts.reshape(-1, tdim), bslot.reshape(-1, 8), kf.value
+    rp, cols = P.csr_host()
+    od, N = orc.dofmap(om, deg)
+    fc, fl = orc.exterior_facets(om)
+    tet_e = [(2, 3), (1, 3), (1, 2), (0, 3), (0, 2), (0, 1)]
+    tri_e = [(1, 2), (0, 2), (0, 1)]
+    E = tet_e if tdim == 3 else tri_e
+    facet_nodes, facet_verts = [], []
+    for c, f in zip(fc, fl):
+        vs = [a for a in range(tdim + 1) if a != f]
+        nodes = {int(od[c, a]) for a in vs}
+        if deg == 2:
+            nodes |= {int(od[c, tdim + 1 + e]) for e, (p, q) in enumerate(E) if f not in (p, q)}
+        facet_nodes.append(nodes)
+        facet_verts.append({int(om.cells[c, a]) for a in vs})
+    expect = {}
+    for i, nodes in enumerate(facet_nodes):
+        for nd in nodes:
+            expect.setdefault(nd, []).append(i)
+    assert sorted(expect) == bnode.tolist()
+    nv = om.nv
+    for t, node in enumerate(bnode):
+        incs = list(range(bptr[t], bptr[t + 1]))
+        assert len(incs) == len(expect[node])
+        for s, i in zip(incs, expect[node]):  # facet-number order
+            got = {int(cols[rp[node] + bslot[s, j]]) for j in range(kf)}
+            assert got == facet_nodes[i]
+            assert set(bverts[s].tolist()) == facet_verts[i]
+            if node < nv:  # vertex row: canonical slot 0, relabelled vertex 0
+                assert cols[rp[node] + bslot[s, 0]] == node and bverts[s, 0] == node
+            else:          # edge row: canonical slot kf-1
+                assert cols[rp[node] + bslot[s, kf - 1]] == node
