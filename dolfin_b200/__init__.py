@@ -14,7 +14,9 @@ numbering with parameters["reorder_dofs_serial"] = False; assembly runs in
 hand-written CUDA kernels reached through the C ABI in include/dolfin_b200.h.
 """
 from . import _capi
-from .assembling import SystemAssembler, assemble, assemble_action, assemble_system
+from .assembling import (SystemAssembler, assemble, assemble_action, assemble_local,
+                         assemble_system)
+from .io import File
 from .bcs import DirichletBC
 from .cpp import (DofMap, FunctionSpace, Mesh, SparsityPattern, UnitCubeMesh, UnitSquareMesh,
                   VectorFunctionSpace, parameters)
@@ -24,7 +26,8 @@ from .ufl import (Identity, SpatialCoordinate, TestFunction, TrialFunction, div,
                   inner, nabla_grad, sym, tr, transpose)
 
 __all__ = [
-    "assemble", "assemble_system", "assemble_action", "SystemAssembler", "Mesh", "UnitCubeMesh",
+    "assemble", "assemble_system", "assemble_action", "assemble_local", "SystemAssembler", "File",
+    "Mesh", "UnitCubeMesh",
     "UnitSquareMesh", "FunctionSpace", "VectorFunctionSpace", "DofMap", "SparsityPattern",
     "parameters", "Function", "Constant", "Matrix", "Vector", "TestFunction", "TrialFunction",
     "grad", "inner", "dot", "dx", "ds", "div", "sym", "tr", "transpose", "nabla_grad", "Identity",

@@ -54,6 +54,10 @@ _SIGS = {
     "db2_mesh_num_exterior_facets": [P, C.POINTER(I64)],
     "db2_mesh_exterior_facets": [P, P, P],
     "db2_mesh_destroy": [P],
+    "db2_mesh_read_xml": [C.c_char_p, PP],
+    "db2_mesh_write_xml": [P, C.c_char_p],
+    "db2_vector_write_xml": [C.c_char_p, I64, P],
+    "db2_vector_read_xml": [C.c_char_p, C.POINTER(I64), P],
     "db2_space_create": [P, I, I, PP],
     "db2_space_info": [P, C.POINTER(I), C.POINTER(I64)],
     "db2_space_cell_dofs": [P, P],
@@ -74,6 +78,7 @@ _SIGS = {
     "db2_assemble_system": [P, P, P, P, P, I, P, P, P],
     "db2_assemble_system_bc": [P, P, P, P, P, P, P, I, P, P, P],
     "db2_assemble_scalar": [P, P, P, P, P],
+    "db2_assemble_local": [P, P, P, P, P, I64, P, P, P],
     "db2_assemble_facets_bc": [P, P, P, P, P, P, P, P, P, P],
     "db2_apply": [P, P, P, I, P, P, P],
     "db2_vjp_kappa": [P, P, P, P, P, P, P, I, P, P],

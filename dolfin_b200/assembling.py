@@ -82,6 +82,40 @@ def assemble(form, tensor=None, form_compiler_parameters=None, add_values=False,
     return b
 
 
+def assemble_local(form, cell):
+    """dolfin.assemble_local (LocalAssembler::assemble,
+    dolfin/fem/LocalAssembler.cpp:39-98): the element tensor of `cell` in its
+    local dof order (cell integral + the cell's exterior-facet integrals), as
+    a numpy array (n, n) or (n,).  `cell` may also be an array of cell
+    indices: then the tensors of all of them, (m, n, n) or (m, n), computed
+    in one launch."""
+    import numpy as np
+    import torch
+    if not isinstance(form, Form):
+        raise TypeError("expected a Form")
+    if form.rank() == 0:
+        raise NotImplementedError("assemble_local of a functional is not provided")
+    cell_rec, facet_rec = recognise_parts(form)
+    rec = cell_rec or facet_rec
+    V = rec.V
+    idx = np.atleast_1d(np.asarray(cell, dtype=np.int64))
+    nc = V.mesh().num_cells()
+    if idx.size and (idx.min() < 0 or idx.max() >= nc):
+        raise IndexError(f"cell index out of range (mesh has {nc} cells)")
+    cells = torch.as_tensor(idx.astype(np.uint32).view(np.int32), device="cuda")
+    n = V._ndofs_cell
+    shape = (idx.size, n, n) if form.rank() == 2 else (idx.size, n)
+    out = torch.empty(shape, dtype=torch.float64, device="cuda")
+    call("db2_assemble_local", V.handle,
+         C.byref(cell_rec.c_form()) if cell_rec is not None else None,
+         _coeff_ptr(cell_rec) if cell_rec is not None else None,
+         C.byref(facet_rec.c_form()) if facet_rec is not None else None,
+         _coeff_ptr(facet_rec) if facet_rec is not None else None,
+         int(idx.size), _ptr(cells), _ptr(out), _stream())
+    res = out.cpu().numpy()
+    return res[0] if np.ndim(cell) == 0 else res
+
+
 def _assemble_scalar(form):
     """double assemble(const Form&) (dolfin/fem/assemble.h:66): the sum of
     the dx and ds parts, each reduced on the device in a fixed order."""

@@ -9,6 +9,7 @@ pattern (dolfin/la/SparsityPattern.h).
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -53,6 +54,11 @@ class Mesh(_Handle):
     _destroy = "db2_mesh_destroy"
 
     def __init__(self, coordinates=None, cells=None, _handle=None):
+        if _handle is None and (isinstance(coordinates, (str, bytes)) or hasattr(coordinates, "__fspath__")):
+            # Mesh("mesh.xml"): DOLFIN XML (dolfin/io/XMLMesh.cpp)
+            h = C.c_void_p()
+            call("db2_mesh_read_xml", os.fsencode(coordinates), C.byref(h))
+            _handle = h
         if _handle is None:
             x = np.ascontiguousarray(coordinates, np.float64)
             c = np.ascontiguousarray(cells, np.uint32)

@@ -150,6 +150,38 @@ int db2_mesh_exterior_facets(db2_mesh m, uint32_t* cell, int32_t* local_facet) {
   });
 }
 
+int db2_mesh_read_xml(const char* path, db2_mesh* out) {
+  return guard([&] {
+    need(path, "path");
+    need(out, "out");
+    *out = new db2_mesh_t{db2::read_mesh_xml(path)};
+  });
+}
+
+int db2_mesh_write_xml(db2_mesh m, const char* path) {
+  return guard([&] {
+    need(m, "mesh");
+    need(path, "path");
+    db2::write_mesh_xml(*m->m, path);
+  });
+}
+
+int db2_vector_write_xml(const char* path, int64_t n, const double* x) {
+  return guard([&] {
+    need(path, "path");
+    need(x, "x");
+    db2::write_vector_xml(path, n, x);
+  });
+}
+
+int db2_vector_read_xml(const char* path, int64_t* n, double* x) {
+  return guard([&] {
+    need(path, "path");
+    need(n, "n");
+    *n = db2::read_vector_xml(path, x, *n);
+  });
+}
+
 int db2_mesh_destroy(db2_mesh m) {
   delete m;
   return DB2_OK;
@@ -332,6 +364,20 @@ int db2_assemble_scalar(db2_mesh m, const db2_form* M, const double* w, double* 
     need(M, "form");
     need(out, "out");
     db2::launch_functional(*m->m, form_args(M, w), out, stream);
+  });
+}
+
+int db2_assemble_local(db2_space V, const db2_form* a, const double* w, const db2_form* a_ds,
+                       const double* w_ds, int64_t ncells, const uint32_t* cells, double* out,
+                       void* stream) {
+  return guard([&] {
+    need(V, "space");
+    need(cells, "cells");
+    need(out, "out");
+    db2::FormArgs fa, fd;
+    if (a) fa = form_args(a, w);
+    if (a_ds) fd = form_args(a_ds, w_ds);
+    db2::launch_local(*V->V, a ? &fa : nullptr, a_ds ? &fd : nullptr, ncells, cells, out, stream);
   });
 }
 

@@ -48,7 +48,7 @@ struct Mesh {
   std::vector<uint32_t> ext_facets;
   // device copies: 4 doubles per vertex (coordinates, then the per-call
   // coefficient values the assembly kernels read with the coordinates)
-  DeviceBuffer d_x, d_cells, d_ext_facets, d_partials;
+  DeviceBuffer d_x, d_cells, d_ext_facets, d_partials, d_ext_mask;
   bool on_device = false;
   void ensure_device();      // first GPU use: upload coordinates and cells
   void upload_coordinates();
@@ -148,6 +148,11 @@ std::shared_ptr<Mesh> make_mesh(int tdim, int64_t nv, const double* x, int64_t n
 std::shared_ptr<Space> make_space(std::shared_ptr<Mesh> m, int degree, int vsize);
 std::shared_ptr<Pattern> make_pattern(std::shared_ptr<Space> V, bool keep_diagonal,
                                       int tile_threads = 0, int seg_cap_bytes = 0);
+// DOLFIN XML files (io.cpp).
+std::shared_ptr<Mesh> read_mesh_xml(const char* path);
+void write_mesh_xml(const Mesh& m, const char* path);
+void write_vector_xml(const char* path, int64_t n, const double* x);
+int64_t read_vector_xml(const char* path, double* x, int64_t cap);  // x NULL: size only
 // Host-side facet plan of a pattern (no device work); Pattern::facet_plan()
 // also uploads it.
 void build_facet_plan(Pattern& P);
@@ -170,6 +175,9 @@ void launch_facet_matrix(Pattern& P, const FormArgs& a, double* vals, bool add_v
 void launch_facet_vector(Pattern& P, const FormArgs& L, double* b, bool add_values,
                          const uint8_t* bc_flags, void* stream);
 void launch_functional(Mesh& m, const FormArgs& M, double* out, void* stream);
+// Element tensors of listed cells (local.cu).
+void launch_local(Space& V, const FormArgs* a, const FormArgs* a_ds, int64_t ncells,
+                  const uint32_t* list, double* out, void* stream);
 void launch_apply(const Pattern& P, const FormArgs& a, int precision, const double* x, double* y,
                   void* stream);
 void launch_vjp(const Pattern& P, const FormArgs& a, const FormArgs& L, int precision,

@@ -116,6 +116,18 @@ int db2_mesh_num_exterior_facets(db2_mesh m, int64_t* n);
 int db2_mesh_exterior_facets(db2_mesh m, uint32_t* cell, int32_t* local_facet);
 int db2_mesh_destroy(db2_mesh m);
 
+/* ---- files (DOLFIN XML; dolfin/io/XMLMesh.cpp, XMLVector.cpp) -------- */
+/* Mesh(filename) / File(filename) >> mesh for a triangle or tetrahedron
+   mesh (dim == tdim); cell vertex lists are sorted, as MeshEditor::close
+   orders a freshly read mesh. */
+int db2_mesh_read_xml(const char* path, db2_mesh* out);
+/* File(filename) << mesh. */
+int db2_mesh_write_xml(db2_mesh m, const char* path);
+/* File(filename) << vector / >> vector for a host array x[n]; read with
+   x = NULL returns the size in *n, else reads at most *n values. */
+int db2_vector_write_xml(const char* path, int64_t n, const double* x);
+int db2_vector_read_xml(const char* path, int64_t* n, double* x);
+
 /* ---- function space + dofmap (DofMap, DofMapBuilder::build) ----------- */
 /* Continuous Lagrange P1/P2 with value_size 1 or tdim; natural UFC
    numbering (DofMapBuilder.cpp:253-272), vector spaces component-major. */
@@ -195,6 +207,17 @@ int db2_assemble_system(db2_pattern P, const db2_form* a, const double* wa, cons
 int db2_assemble_system_bc(db2_pattern P, const db2_form* a, const double* wa, const db2_form* L,
                            const double* wL, const uint8_t* bc_flags, const double* bc_vals,
                            int precision, double* vals, double* b, void* stream);
+/* assemble_local (LocalAssembler::assemble, dolfin/fem/LocalAssembler.cpp:
+   39-98) for a list of cells: the dense tensor of each cell in its local
+   dof order (DofMap::cell_dofs order; vector spaces component-major),
+   row-major over (test, trial): out[ncells*n*n] (bilinear) or out[ncells*n]
+   (linear), n = dofs per cell, device.  a: the cell integral (diffusion,
+   elasticity or load) and/or a_ds: the exterior-facet integral, added for
+   the facets of each cell that lie on the boundary.  cells: device
+   uint32[ncells]; an index beyond the mesh leaves its tensor unwritten. */
+int db2_assemble_local(db2_space V, const db2_form* a, const double* w, const db2_form* a_ds,
+                       const double* w_ds, int64_t ncells, const uint32_t* cells, double* out,
+                       void* stream);
 /* The exterior-facet terms of a SystemAssembler pass with DirichletBC
    (SystemAssembler.cpp:417-470 adds them to the cell tensor before
    apply_bc): call after db2_assemble_system_bc with the same bc_flags /
