@@ -59,6 +59,8 @@ _SIGS = {
     "db2_vector_write_xml": [C.c_char_p, I64, P],
     "db2_vector_read_xml": [C.c_char_p, C.POINTER(I64), P],
     "db2_space_create": [P, I, I, PP],
+    "db2_space_create_reordered": [P, I, I, PP],
+    "db2_space_node_numbers": [P, P],
     "db2_space_info": [P, C.POINTER(I), C.POINTER(I64)],
     "db2_space_cell_dofs": [P, P],
     "db2_space_destroy": [P],

@@ -36,7 +36,7 @@ def _coeff_ptr(rec):
     f = rec.function
     if f.function_space().mesh() is not rec.V.mesh():
         raise ValueError("coefficient and form live on different meshes")
-    return _ptr(f.tensor())
+    return _ptr(f.vertex_tensor())
 
 
 def _check_tensor_dims(tensor, rec):
@@ -126,7 +126,7 @@ def _assemble_scalar(form):
         if func is not None:
             if func.function_space().mesh() is not mesh:
                 raise ValueError("coefficient and form live on different meshes")
-            w = _ptr(func.tensor())
+            w = _ptr(func.vertex_tensor())
         out = torch.empty(1, dtype=torch.float64, device="cuda")
         call("db2_assemble_scalar", mesh.handle, C.byref(_capi.make_form(kind, coeff, const)), w,
              _ptr(out), _stream())

@@ -72,8 +72,13 @@ class DirichletBC:
         cd = V.dofmap().cell_dofs_all()
         vs = V.value_size()
         k = cd.shape[1] // vs
-        nodes = cd[:, :k]  # component-0 dofs are the node numbers
         nn = V.dim() // vs
+        # natural node numbers of the cells (vertices, then nv + edge index)
+        if V.reordered():
+            inv = np.argsort(V.node_numbers())
+            nodes = inv[cd[:, :k] // vs]
+        else:
+            nodes = cd[:, :k]  # component-0 dofs are the node numbers
         bnodes = set()
         edges = _TET_EDGES if tdim == 3 else _TRI_EDGES
         for c, a in zip(owner, local):
@@ -97,7 +102,7 @@ class DirichletBC:
                     allpts[nodes[:, nv_cell + e]] = 0.5 * (x[nodes[:, p]] + x[nodes[:, q]])
             pts = allpts[bn]
         vals = self._values(pts, vs, bn.size)
-        dofs = np.concatenate([c * nn + bn for c in range(vs)])
+        dofs = np.concatenate([V.node_dofs(c, bn) for c in range(vs)])
         values = np.concatenate([vals[:, c] for c in range(vs)])
         self._cache = (dofs, values)
         return self._cache

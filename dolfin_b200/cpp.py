@@ -183,12 +183,12 @@ class FunctionSpace(_Handle):
     def __init__(self, mesh, family="Lagrange", degree=1, value_size=1):
         if family not in _FAMILIES:
             raise NotImplementedError(f"family {family!r}: only continuous Lagrange is provided")
-        if parameters.get("reorder_dofs_serial", False):
-            raise NotImplementedError(
-                "reorder_dofs_serial=True (RCM dof reordering) is not provided; set "
-                "parameters['reorder_dofs_serial'] = False")
+        # reorder_dofs_serial = True: the reference's reverse Cuthill-McKee
+        # numbering (dof_ordering_library "Boost"), dofs bs*node + c
+        self._reordered = bool(parameters.get("reorder_dofs_serial", False))
         h = C.c_void_p()
-        call("db2_space_create", mesh.handle, int(degree), int(value_size), C.byref(h))
+        call("db2_space_create_reordered" if self._reordered else "db2_space_create",
+             mesh.handle, int(degree), int(value_size), C.byref(h))
         super().__init__(h)
         self._mesh = mesh
         self._degree = int(degree)
@@ -204,6 +204,24 @@ class FunctionSpace(_Handle):
 
     def dim(self):
         return self._dim
+
+    def reordered(self):
+        return self._reordered
+
+    def node_numbers(self):
+        """Number of each natural node (vertex index, then nv + edge index)."""
+        if getattr(self, "_node_new", None) is None:
+            out = np.empty(self._dim // self._vs, np.int32)
+            call("db2_space_node_numbers", self._h, _ptr(out))
+            self._node_new = out
+        return self._node_new
+
+    def node_dofs(self, comp, nodes):
+        """Dofs of component `comp` at natural nodes `nodes`."""
+        nodes = np.asarray(nodes, np.int64)
+        if self._reordered:
+            return self._vs * self.node_numbers()[nodes].astype(np.int64) + comp
+        return comp * (self._dim // self._vs) + nodes
 
     def degree(self):
         return self._degree

@@ -187,6 +187,7 @@ int db2_batch_create(int count, const db2_pattern* patterns, const db2_form* for
       for (int m = 0; m < count; ++m) {
         auto P = pattern_of(patterns[m]);
         if (!P) fail(DB2_ERR_ARGUMENT, "batch member %d: NULL pattern", m);
+        if (P->V->reordered()) fail(DB2_ERR_UNSUPPORTED, "batch member %d: reordered space", m);
         if (forms[m].kind != DB2_FORM_DIFFUSION || forms[m].coeff != DB2_COEFF_P1 || P->bs != 1)
           fail(DB2_ERR_UNSUPPORTED, "batch member %d: only kappa*grad.grad with a P1 kappa", m);
         if (!kappas[m] || !vals[m]) fail(DB2_ERR_ARGUMENT, "batch member %d: NULL kappa/vals", m);

@@ -23,6 +23,12 @@ struct db2_pattern_t {
 
 namespace db2 {
 int64_t launches();
+ReorderedCSR& reordered_on_device(Pattern& P);
+void gather_values(Pattern& P, double* vals, bool add, void* stream);
+void gather_dofs(Pattern& P, double* dst, const double* src_nat, bool add, void* stream);
+void scatter_dofs(Pattern& P, double* dst_nat, const double* src, void* stream);
+void scatter_flags(Pattern& P, uint8_t* dst_nat, const uint8_t* src, void* stream);
+void scatter_values(Pattern& P, double* dst_nat, const double* src, void* stream);
 std::shared_ptr<Pattern> pattern_of(db2_pattern P) { return P ? P->P : nullptr; }
 }
 
@@ -195,6 +201,25 @@ int db2_space_create(db2_mesh m, int degree, int value_size, db2_space* out) {
   });
 }
 
+int db2_space_create_reordered(db2_mesh m, int degree, int value_size, db2_space* out) {
+  return guard([&] {
+    need(m, "mesh");
+    need(out, "out");
+    auto V = db2::make_space(m->m, degree, value_size);
+    V->node_new = db2::rcm_node_order(*V);
+    *out = new db2_space_t{V};
+  });
+}
+
+int db2_space_node_numbers(db2_space V, int32_t* node_new) {
+  return guard([&] {
+    need(V, "space");
+    need(node_new, "node_new");
+    const auto& S = *V->V;
+    for (int64_t i = 0; i < S.nnodes; ++i) node_new[i] = S.reordered() ? S.node_new[i] : int32_t(i);
+  });
+}
+
 int db2_space_info(db2_space V, int* ndofs_per_cell, int64_t* dim) {
   return guard([&] {
     need(V, "space");
@@ -213,7 +238,7 @@ int db2_space_cell_dofs(db2_space V, int32_t* out) {
     for (int64_t c = 0; c < S.mesh->nc; ++c)
       for (int comp = 0; comp < S.vsize; ++comp)
         for (int i = 0; i < k; ++i)
-          out[c * n + comp * k + i] = int32_t(comp * S.nnodes + S.cell_nodes[c * k + i]);
+          out[c * n + comp * k + i] = int32_t(S.dof(comp, S.cell_nodes[c * k + i]));
   });
 }
 
@@ -249,6 +274,12 @@ int db2_pattern_csr_device(db2_pattern P, const int32_t** rowptr, const int32_t*
   return guard([&] {
     need(P, "pattern");
     P->P->ensure_device();
+    if (P->P->V->reordered()) {
+      db2::ReorderedCSR& R = db2::reordered_on_device(*P->P);
+      if (rowptr) *rowptr = R.d_rowptr.as<int32_t>();
+      if (cols) *cols = R.d_cols.as<int32_t>();
+      return;
+    }
     if (rowptr) *rowptr = P->P->d_rowptr.as<int32_t>();
     if (cols) *cols = P->P->d_cols.as<int32_t>();
   });
@@ -334,11 +365,16 @@ int db2_assemble_matrix(db2_pattern P, const db2_form* a, const double* w, int p
     need(a, "form");
     need(vals, "vals");
     const db2::FormArgs fa = form_args(a, w);
+    db2::Pattern& Pt = *P->P;
+    // reordered space: assemble in natural order into scratch, then gather
+    const bool ro = Pt.V->reordered();
+    double* out = ro ? db2::reordered_on_device(Pt).d_vals.as<double>() : vals;
+    const bool add = ro ? false : add_values != 0;
     if (a->kind == DB2_FORM_FACET_MASS)
-      db2::launch_facet_matrix(*P->P, fa, vals, add_values != 0, nullptr, nullptr, nullptr, stream);
+      db2::launch_facet_matrix(Pt, fa, out, add, nullptr, nullptr, nullptr, stream);
     else
-      db2::launch_assemble(*P->P, &fa, nullptr, precision, vals, nullptr, add_values != 0, nullptr,
-                           nullptr, stream);
+      db2::launch_assemble(Pt, &fa, nullptr, precision, out, nullptr, add, nullptr, nullptr, stream);
+    if (ro) db2::gather_values(Pt, vals, add_values != 0, stream);
   });
 }
 
@@ -349,11 +385,15 @@ int db2_assemble_vector(db2_pattern P, const db2_form* L, const double* w, doubl
     need(L, "form");
     need(b, "b");
     const db2::FormArgs fl = form_args(L, w);
+    db2::Pattern& Pt = *P->P;
+    const bool ro = Pt.V->reordered();
+    double* out = ro ? db2::reordered_on_device(Pt).d_b.as<double>() : b;
+    const bool add = ro ? false : add_values != 0;
     if (L->kind == DB2_FORM_FACET_LOAD)
-      db2::launch_facet_vector(*P->P, fl, b, add_values != 0, nullptr, stream);
+      db2::launch_facet_vector(Pt, fl, out, add, nullptr, stream);
     else
-      db2::launch_assemble(*P->P, nullptr, &fl, DB2_FP64, nullptr, b, add_values != 0, nullptr,
-                           nullptr, stream);
+      db2::launch_assemble(Pt, nullptr, &fl, DB2_FP64, nullptr, out, add, nullptr, nullptr, stream);
+    if (ro) db2::gather_dofs(Pt, b, out, add_values != 0, stream);
   });
 }
 
@@ -389,11 +429,30 @@ int db2_assemble_facets_bc(db2_pattern P, const db2_form* a_ds, const double* wa
     need(bc_flags, "bc_flags");
     need(bc_vals, "bc_vals");
     need(b, "b");
-    if (a_ds) {
-      need(vals, "vals");
-      db2::launch_facet_matrix(*P->P, form_args(a_ds, wa), vals, true, bc_flags, bc_vals, b, stream);
+    db2::Pattern& Pt = *P->P;
+    if (a_ds) need(vals, "vals");
+    if (Pt.V->reordered()) {
+      // natural scratch from zero, the facet terms added there, then gathered
+      // and added to the caller's arrays
+      db2::ReorderedCSR& R = db2::reordered_on_device(Pt);
+      cudaStream_t s = static_cast<cudaStream_t>(stream);
+      db2::scatter_flags(Pt, R.d_flags.as<uint8_t>(), bc_flags, stream);
+      db2::scatter_dofs(Pt, R.d_bcv.as<double>(), bc_vals, stream);
+      cudaMemsetAsync(R.d_b.ptr, 0, size_t(Pt.V->dim()) * sizeof(double), s);
+      if (a_ds) {
+        cudaMemsetAsync(R.d_vals.ptr, 0, size_t(Pt.nnz) * sizeof(double), s);
+        db2::launch_facet_matrix(Pt, form_args(a_ds, wa), R.d_vals.as<double>(), true,
+                                 R.d_flags.as<uint8_t>(), R.d_bcv.as<double>(), R.d_b.as<double>(), stream);
+        db2::gather_values(Pt, vals, true, stream);
+      }
+      if (L_ds)
+        db2::launch_facet_vector(Pt, form_args(L_ds, wL), R.d_b.as<double>(), true,
+                                 R.d_flags.as<uint8_t>(), stream);
+      db2::gather_dofs(Pt, b, R.d_b.as<double>(), true, stream);
+      return;
     }
-    if (L_ds) db2::launch_facet_vector(*P->P, form_args(L_ds, wL), b, true, bc_flags, stream);
+    if (a_ds) db2::launch_facet_matrix(Pt, form_args(a_ds, wa), vals, true, bc_flags, bc_vals, b, stream);
+    if (L_ds) db2::launch_facet_vector(Pt, form_args(L_ds, wL), b, true, bc_flags, stream);
   });
 }
 
@@ -406,7 +465,16 @@ int db2_assemble_system(db2_pattern P, const db2_form* a, const double* wa, cons
     need(vals, "vals");
     need(b, "b");
     const db2::FormArgs fa = form_args(a, wa), fl = form_args(L, wL);
-    db2::launch_assemble(*P->P, &fa, &fl, precision, vals, b, false, nullptr, nullptr, stream);
+    db2::Pattern& Pt = *P->P;
+    if (Pt.V->reordered()) {
+      db2::ReorderedCSR& R = db2::reordered_on_device(Pt);
+      db2::launch_assemble(Pt, &fa, &fl, precision, R.d_vals.as<double>(), R.d_b.as<double>(), false,
+                           nullptr, nullptr, stream);
+      db2::gather_values(Pt, vals, false, stream);
+      db2::gather_dofs(Pt, b, R.d_b.as<double>(), false, stream);
+      return;
+    }
+    db2::launch_assemble(Pt, &fa, &fl, precision, vals, b, false, nullptr, nullptr, stream);
   });
 }
 
@@ -420,7 +488,18 @@ int db2_assemble_system_bc(db2_pattern P, const db2_form* a, const double* wa, c
     need(bc_flags, "bc_flags");
     need(bc_vals, "bc_vals");
     const db2::FormArgs fa = form_args(a, wa), fl = form_args(L, wL);
-    db2::launch_assemble(*P->P, &fa, &fl, precision, vals, b, false, bc_flags, bc_vals, stream);
+    db2::Pattern& Pt = *P->P;
+    if (Pt.V->reordered()) {
+      db2::ReorderedCSR& R = db2::reordered_on_device(Pt);
+      db2::scatter_flags(Pt, R.d_flags.as<uint8_t>(), bc_flags, stream);
+      db2::scatter_dofs(Pt, R.d_bcv.as<double>(), bc_vals, stream);
+      db2::launch_assemble(Pt, &fa, &fl, precision, R.d_vals.as<double>(), R.d_b.as<double>(), false,
+                           R.d_flags.as<uint8_t>(), R.d_bcv.as<double>(), stream);
+      db2::gather_values(Pt, vals, false, stream);
+      db2::gather_dofs(Pt, b, R.d_b.as<double>(), false, stream);
+      return;
+    }
+    db2::launch_assemble(Pt, &fa, &fl, precision, vals, b, false, bc_flags, bc_vals, stream);
   });
 }
 
@@ -431,7 +510,15 @@ int db2_apply(db2_pattern P, const db2_form* a, const double* w, int precision, 
     need(a, "form");
     need(x, "x");
     need(y, "y");
-    db2::launch_apply(*P->P, form_args(a, w), precision, x, y, stream);
+    db2::Pattern& Pt = *P->P;
+    if (Pt.V->reordered()) {
+      db2::ReorderedCSR& R = db2::reordered_on_device(Pt);
+      db2::scatter_dofs(Pt, R.d_vec.as<double>(), x, stream);
+      db2::launch_apply(Pt, form_args(a, w), precision, R.d_vec.as<double>(), R.d_b.as<double>(), stream);
+      db2::gather_dofs(Pt, y, R.d_b.as<double>(), false, stream);
+      return;
+    }
+    db2::launch_apply(Pt, form_args(a, w), precision, x, y, stream);
   });
 }
 
@@ -453,7 +540,16 @@ int db2_vjp_kappa(db2_pattern P, const db2_form* a, const double* kappa, const d
       fl.f.kind = DB2_FORM_LOAD;
       fl.f.coeff = DB2_COEFF_NONE;
     }
-    db2::launch_vjp(*P->P, form_args(a, kappa), fl, precision, gA, L ? gb : nullptr, dkappa,
+    db2::Pattern& Pt = *P->P;
+    if (Pt.V->reordered()) {
+      // upstream gradients into the natural numbering
+      db2::ReorderedCSR& R = db2::reordered_on_device(Pt);
+      db2::scatter_values(Pt, R.d_vals.as<double>(), gA, stream);
+      if (L && gb) db2::scatter_dofs(Pt, R.d_b.as<double>(), gb, stream);
+      gA = R.d_vals.as<double>();
+      if (L && gb) gb = R.d_b.as<double>();
+    }
+    db2::launch_vjp(Pt, form_args(a, kappa), fl, precision, gA, L ? gb : nullptr, dkappa,
                     P->scratch.as<double>(), stream);
   });
 }

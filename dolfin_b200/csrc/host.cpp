@@ -706,7 +706,17 @@ void Pattern::ensure_device() {
   on_device = true;
 }
 
-void Pattern::csr_host(int32_t* rowptr, int32_t* cols) const {
+void Pattern::csr_host(int32_t* rowptr, int32_t* cols) {
+  if (!V->reordered()) {
+    csr_host_natural(rowptr, cols);
+    return;
+  }
+  if (!reordered.built) build_reordered_csr(*this);
+  if (rowptr) std::copy(reordered.rowptr.begin(), reordered.rowptr.end(), rowptr);
+  if (cols) std::copy(reordered.cols.begin(), reordered.cols.end(), cols);
+}
+
+void Pattern::csr_host_natural(int32_t* rowptr, int32_t* cols) const {
   const int64_t nn = V->nnodes;
   for (int c = 0; c < bs; ++c)
     for (int64_t i = 0; i < nn; ++i) {

@@ -65,7 +65,15 @@ struct Space {
   int degree = 1, vsize = 1;
   int k = 0;              // nodes (scalar dofs) per cell
   int64_t nnodes = 0;     // scalar global dimension
-  std::vector<uint32_t> cell_nodes;  // nc * k
+  std::vector<uint32_t> cell_nodes;  // nc * k (natural node numbering)
+  // reorder_dofs_serial = True: node_new[node] = reverse Cuthill-McKee number
+  // of a (natural) node; dofs are then bs * node_new[node] + c.  Empty for the
+  // natural numbering, where dofs are c * nnodes + node.
+  std::vector<int32_t> node_new;
+  bool reordered() const { return !node_new.empty(); }
+  int64_t dof(int c, int64_t node) const {
+    return reordered() ? int64_t(vsize) * node_new[node] + c : int64_t(c) * nnodes + node;
+  }
   DeviceBuffer d_cell_nodes;
   DeviceBuffer d_edge_vertices;      // P2: sorted endpoints of each edge node
   bool on_device = false;
@@ -98,6 +106,16 @@ struct FacetPlan {
   DeviceBuffer d_bnode, d_binc_ptr, d_bverts, d_bslot;
 };
 
+// CSR of a pattern on a reordered space, in the space's numbering.  The
+// kernels assemble in the natural numbering (into library scratch) and
+// gather: vals[k] = natural_vals[val_src[k]], b[i] = natural_b[dof_src[i]].
+struct ReorderedCSR {
+  bool built = false;
+  std::vector<int32_t> rowptr, cols, val_src, dof_src;
+  DeviceBuffer d_rowptr, d_cols, d_val_src, d_dof_src;
+  DeviceBuffer d_vals, d_b, d_flags, d_bcv, d_vec;  // natural-order scratch
+};
+
 struct Pattern {
   std::shared_ptr<Space> V;
   bool keep_diagonal = false;
@@ -128,8 +146,11 @@ struct Pattern {
   DeviceBuffer d_node_rowptr, d_inc_ptr, d_inc, d_rec, d_rec_goff, d_cell_inc, d_tiles, d_rowptr, d_cols;
   bool on_device = false;
   void ensure_device();      // first GPU use: upload the plan, expand the CSR
-  // dof-level CSR on the host (component expansion of the node graph)
-  void csr_host(int32_t* rowptr, int32_t* cols) const;
+  // dof-level CSR on the host in the natural numbering (component expansion
+  // of the node graph) and in the space's numbering (reordered if it is)
+  void csr_host_natural(int32_t* rowptr, int32_t* cols) const;
+  void csr_host(int32_t* rowptr, int32_t* cols);
+  ReorderedCSR reordered;
   std::unique_ptr<FacetPlan> facets;
   const FacetPlan& facet_plan();     // built and uploaded on first use
 };
@@ -148,6 +169,10 @@ std::shared_ptr<Mesh> make_mesh(int tdim, int64_t nv, const double* x, int64_t n
 std::shared_ptr<Space> make_space(std::shared_ptr<Mesh> m, int degree, int vsize);
 std::shared_ptr<Pattern> make_pattern(std::shared_ptr<Space> V, bool keep_diagonal,
                                       int tile_threads = 0, int seg_cap_bytes = 0);
+// Reordered numbering (reorder_host.cpp): RCM number of each natural node; the
+// reordered CSR of a pattern.
+std::vector<int32_t> rcm_node_order(const Space& V);
+void build_reordered_csr(Pattern& P);
 // DOLFIN XML files (io.cpp).
 std::shared_ptr<Mesh> read_mesh_xml(const char* path);
 void write_mesh_xml(const Mesh& m, const char* path);

@@ -67,6 +67,10 @@ extern "C" int db2_vjp_kappa_noalloc(db2_pattern Ph, const db2_form* a, const do
            "db2_vjp_kappa_noalloc needs %zu scratch doubles but its fixed array holds %zu "
            "(at most 524288 tetrahedra / 699050 triangles); use db2_vjp_kappa",
            need, kNoAllocScratchDoubles);
+    if (P->V->reordered())
+      fail(DB2_ERR_UNSUPPORTED,
+           "db2_vjp_kappa_noalloc does not take patterns on reordered spaces (their gradients "
+           "need library scratch); use db2_vjp_kappa");
     if (!P->on_device)
       fail(DB2_ERR_ARGUMENT,
            "pattern is not resident on the device yet; assemble with it (or call "

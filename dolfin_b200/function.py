@@ -67,6 +67,19 @@ class Function(Expr):
         """The device dof vector (torch float64)."""
         return self._x
 
+    def vertex_tensor(self):
+        """Values by vertex index of a P1 function (the engine's coefficient
+        layout): the dof vector itself, or gathered for a reordered space.
+        The gathered copy is kept on the object so that it outlives the
+        asynchronous kernels that read it."""
+        V = self._V
+        if not V.reordered():
+            return self._x
+        import torch
+        idx = torch.as_tensor(V.node_numbers().astype("int64"), device=self._x.device)
+        self._vtx = self._x[idx]
+        return self._vtx
+
     def assign_values(self, values):
         import torch
         self._x.copy_(torch.as_tensor(values, dtype=torch.float64))

@@ -132,6 +132,18 @@ int db2_vector_read_xml(const char* path, int64_t* n, double* x);
 /* Continuous Lagrange P1/P2 with value_size 1 or tdim; natural UFC
    numbering (DofMapBuilder.cpp:253-272), vector spaces component-major. */
 int db2_space_create(db2_mesh m, int degree, int value_size, db2_space* out);
+/* The same space with the reordered numbering of reorder_dofs_serial = True
+   and dof_ordering_library = "Boost" (DofMapBuilder.cpp:168-252,
+   compute_node_reordering :1473-1667, BoostGraphOrdering.cpp:34-75): nodes
+   numbered by reverse Cuthill-McKee of the node graph, dofs bs*node + c.
+   Matrices, vectors, Dirichlet arrays and gradients passed with a pattern
+   of this space are in this numbering (the engine assembles in the natural
+   numbering into library scratch -- nnz + 3 N doubles -- and gathers);
+   coefficient fields stay vertex-indexed. */
+int db2_space_create_reordered(db2_mesh m, int degree, int value_size, db2_space* out);
+/* node_new[nnodes]: the number of each natural node (identity unless
+   reordered); natural node = vertex index, then nv + edge index. */
+int db2_space_node_numbers(db2_space V, int32_t* node_new);
 int db2_space_info(db2_space V, int* ndofs_per_cell, int64_t* dim);
 /* DofMap::cell_dofs for all cells (dolfin/fem/DofMap.h:201-206), host out[nc*ndofs]. */
 int db2_space_cell_dofs(db2_space V, int32_t* out);

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <memory>
 #include <numeric>
 #include <stdexcept>
@@ -775,6 +776,150 @@ int64_t orc_dofmap(int family, int degree, int vsize, int tdim, int64_t nv, int6
       for (int i = 0; i < k; ++i) cell_dofs[c * n + comp * k + i] = (int32_t)(comp * nscalar + sd[i]);
   }
   return nscalar * vsize;
+}
+
+// ---- reordered dofmap -------------------------------------------------------
+// DofMapBuilder::compute_node_reordering (dolfin/fem/DofMapBuilder.cpp:
+// 1473-1667) on one process: graph[n0].insert(n1) for every ordered pair of
+// distinct nodes of every cell (dolfin::Set, dolfin/common/Set.h:79-96), then
+// BoostGraphOrdering::compute_cuthill_mckee(graph, true)
+// (dolfin/graph/BoostGraphOrdering.cpp:34-75), then build_dofmap (:1669-1693):
+// dof = bs*new_node + component.  The Boost algorithm (not in the reference
+// tree) is restated after boost/graph/cuthill_mckee_ordering.hpp and
+// sparse_ordering.hpp: rcm_queue-style level bookkeeping for the
+// pseudo-peripheral search, and a BFS whose visitor sorts the vertices it
+// enqueued for each examined vertex by degree.
+namespace {
+
+struct LevelQueue {  // Boost's rcm_queue
+  std::deque<int32_t> q;
+  const std::vector<int32_t>* deg;
+  size_t in_level = 0, level_size = 1;
+  int ecc = -1;
+  int32_t spouse = -1;
+  int32_t front() {
+    const int32_t u = q.front();
+    if (in_level == 0) spouse = u;
+    else if ((*deg)[u] < (*deg)[spouse]) spouse = u;
+    return u;
+  }
+  void pop() {
+    if (!in_level) level_size = q.size();
+    q.pop_front();
+    if (in_level == level_size - 1) {
+      in_level = 0;
+      ++ecc;
+    } else {
+      ++in_level;
+    }
+  }
+};
+
+int32_t peripheral_pair(const std::vector<std::vector<int32_t>>& g, const std::vector<int32_t>& deg,
+                        int32_t u, int& ecc) {
+  std::vector<uint8_t> seen(g.size(), 0);
+  LevelQueue Q;
+  Q.deg = &deg;
+  Q.q.push_back(u);
+  seen[u] = 1;
+  while (!Q.q.empty()) {
+    const int32_t x = Q.front();
+    Q.pop();
+    for (int32_t y : g[x])
+      if (!seen[y]) {
+        seen[y] = 1;
+        Q.q.push_back(y);
+      }
+  }
+  ecc = Q.ecc;
+  return Q.spouse;
+}
+
+std::vector<int32_t> boost_rcm(const std::vector<std::vector<int32_t>>& g) {
+  const int32_t n = (int32_t)g.size();
+  std::vector<int32_t> deg(n);
+  for (int32_t v = 0; v < n; ++v) deg[v] = (int32_t)g[v].size();
+  std::vector<int32_t> map(n);
+  bool any = false;
+  for (int32_t v = 0; v < n; ++v) any |= !g[v].empty();
+  if (!any) {
+    for (int32_t v = 0; v < n; ++v) map[v] = v;
+    return map;
+  }
+  // one vertex per component, in vertex order (depth_first_visit from each
+  // still-white vertex)
+  std::vector<uint8_t> col(n, 0);
+  std::vector<int32_t> comp;
+  for (int32_t v = 0; v < n; ++v) {
+    if (col[v]) continue;
+    comp.push_back(v);
+    std::vector<int32_t> st{v};
+    col[v] = 1;
+    while (!st.empty()) {
+      const int32_t u = st.back();
+      st.pop_back();
+      for (int32_t w : g[u])
+        if (!col[w]) { col[w] = 1; st.push_back(w); }
+    }
+  }
+  for (int32_t& r : comp) {  // find_starting_node
+    int er, ex;
+    int32_t x = peripheral_pair(g, deg, r, er);
+    int32_t y = peripheral_pair(g, deg, x, ex);
+    while (ex > er) {
+      r = x;
+      er = ex;
+      x = y;
+      y = peripheral_pair(g, deg, x, ex);
+    }
+    r = x;
+  }
+  std::vector<uint8_t> color(n, 0);  // white 0, gray 1, black 2
+  std::vector<int32_t> perm;         // visit order
+  std::deque<int32_t> Q;
+  for (int32_t s : comp) {
+    color[s] = 1;
+    Q.push_back(s);
+    while (!Q.empty()) {
+      const int32_t u = Q.front();
+      Q.pop_front();
+      perm.push_back(u);                       // examine_vertex
+      const size_t first_child = Q.size();
+      for (int32_t v : g[u])
+        if (color[v] == 0) { color[v] = 1; Q.push_back(v); }
+      color[u] = 2;
+      std::sort(Q.begin() + first_child, Q.end(),   // finish_vertex
+                [&](int32_t a, int32_t b) { return deg[a] < deg[b]; });
+    }
+  }
+  // written through inv_perm.rbegin(), then map[inv_perm[i]] = i
+  for (int32_t i = 0; i < n; ++i) map[perm[i]] = n - 1 - i;
+  return map;
+}
+
+}  // namespace
+
+int64_t orc_dofmap_reordered(int degree, int vsize, int tdim, int64_t nv, int64_t nc,
+                             const uint32_t* cells, int32_t* cell_dofs, int32_t* node_new) {
+  const int k = scalar_dim(ORC_CG, degree, tdim);
+  std::vector<int32_t> nodes((size_t)nc * k);
+  const int64_t nn = orc_dofmap(ORC_CG, degree, 1, tdim, nv, nc, cells, nodes.data());
+  std::vector<std::vector<int32_t>> g(nn);
+  for (int64_t c = 0; c < nc; ++c)
+    for (int i = 0; i < k; ++i)
+      for (int j = 0; j < k; ++j) {
+        if (i == j) continue;
+        std::vector<int32_t>& set = g[nodes[c * k + i]];
+        const int32_t x = nodes[c * k + j];
+        if (std::find(set.begin(), set.end(), x) == set.end()) set.push_back(x);
+      }
+  const std::vector<int32_t> map = boost_rcm(g);
+  for (int64_t c = 0; c < nc; ++c)
+    for (int i = 0; i < k; ++i)
+      for (int b = 0; b < vsize; ++b)
+        cell_dofs[c * k * vsize + b * k + i] = vsize * map[nodes[c * k + i]] + b;
+  if (node_new) std::copy(map.begin(), map.end(), node_new);
+  return nn * vsize;
 }
 
 // SparsityPatternBuilder::build over cells (dolfin/fem/SparsityPatternBuilder.cpp:94-111)

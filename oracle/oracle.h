@@ -90,6 +90,12 @@ int64_t orc_dofmap(int family, int degree, int vsize, int tdim,
                    int64_t nv, int64_t nc, const uint32_t* cells,
                    int32_t* cell_dofs);
 int orc_ndofs_per_cell(int family, int degree, int vsize, int tdim);
+/* DofMapBuilder::build with reorder_dofs_serial = true and
+   dof_ordering_library = "Boost" (CG only): node graph with dolfin::Set
+   insertion, Boost's reverse Cuthill-McKee, dofs bs*node + c.  node_new may
+   be NULL. */
+int64_t orc_dofmap_reordered(int degree, int vsize, int tdim, int64_t nv, int64_t nc,
+                             const uint32_t* cells, int32_t* cell_dofs, int32_t* node_new);
 
 /* ---- sparsity (SparsityPatternBuilder::build + EigenMatrix::init) ----- */
 typedef struct orc_csr orc_csr;

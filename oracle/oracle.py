@@ -57,6 +57,8 @@ def lib():
         L.orc_dofmap.argtypes = [i32, i32, i32, i32, i64, i64, P, P]
         L.orc_dofmap.restype = i64
         L.orc_ndofs_per_cell.argtypes = [i32, i32, i32, i32]
+        L.orc_dofmap_reordered.argtypes = [i32, i32, i32, i64, i64, P, P, P]
+        L.orc_dofmap_reordered.restype = i64
         L.orc_sparsity.argtypes = [i64, i64, i64, i32, P, i32, P, i32]
         L.orc_sparsity.restype = P
         L.orc_csr_nnz.argtypes = [P]
@@ -155,6 +157,18 @@ def dofmap(mesh, degree, vsize=1, family=CG):
     cells = np.ascontiguousarray(mesh.cells)
     n = lib().orc_dofmap(family, degree, vsize, mesh.tdim, mesh.nv, mesh.nc, _p(cells), _p(out))
     return out, int(n)
+
+
+def dofmap_reordered(mesh, degree, vsize=1):
+    """reorder_dofs_serial = True (Boost RCM): (cell dofs, dimension, node_new)."""
+    k = lib().orc_ndofs_per_cell(CG, degree, vsize, mesh.tdim)
+    out = np.empty((mesh.nc, k), np.int32)
+    cells = np.ascontiguousarray(mesh.cells)
+    nn = (mesh.nv + (edges(mesh)[1].shape[0] if degree == 2 else 0))
+    node_new = np.empty(nn, np.int32)
+    n = lib().orc_dofmap_reordered(degree, vsize, mesh.tdim, mesh.nv, mesh.nc, _p(cells), _p(out),
+                                   _p(node_new))
+    return out, int(n), node_new
 
 
 def sparsity(nrows, ncols, dofs0, dofs1, keep_diagonal=False):
