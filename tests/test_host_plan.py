@@ -1,6 +1,8 @@
 """Host-side parity (no GPU): meshes, entity numbering, dofmaps and the
 sparsity pattern of the engine are bit-identical to the oracle's
 restatement of DOLFIN; the row-gather plan is self-consistent."""
+import os
+
 import numpy as np
 import pytest
 
@@ -229,3 +231,26 @@ def test_facet_plan_slots_point_at_the_facet_nodes(orc, tdim, deg):
                 assert cols[rp[node] + bslot[s, 0]] == node and bverts[s, 0] == node
             else:          # edge row: canonical slot kf-1
                 assert cols[rp[node] + bslot[s, kf - 1]] == node
+
+
+def test_new_entry_points_reject_bad_arguments():
+    # checked on the host before any device work: status codes, not crashes
+    import ctypes as C
+    m = d2.UnitCubeMesh(1, 1, 1)
+    V = d2.FunctionSpace(m, "Lagrange", 1)
+    P = V.pattern()
+    lib = _capi.lib()
+    f = _capi.make_form(_capi.FORM_FUNCTIONAL, _capi.COEFF_CONSTANT, (1.0,))
+    assert lib.db2_assemble_scalar(None, C.byref(f), None, None, None) == 1
+    assert lib.db2_assemble_scalar(m.handle, C.byref(f), None, None, None) == 1  # out NULL
+    assert lib.db2_assemble_local(V.handle, None, None, None, None, 1, None, None, None) == 1
+    assert lib.db2_assemble_facets_bc(P.handle, None, None, None, None, None, None, None, None, None) == 1
+    assert lib.db2_vector_write_xml(b"/nonexistent_dir/x.xml", 3, None) == 1
+    n = C.c_int64(0)
+    assert lib.db2_vector_read_xml(b"/nonexistent_dir/x.xml", C.byref(n), None) == 1
+    assert lib.db2_mesh_write_xml(None, b"x.xml") == 1
+    with pytest.raises(NotImplementedError):
+        d2.assemble(d2.inner(d2.grad(d2.TrialFunction(V)), d2.grad(d2.TestFunction(V))) * d2.ds)
+    with pytest.raises(NotImplementedError):
+        d2.assemble_action(d2.TrialFunction(V) * d2.TestFunction(V) * d2.ds, d2.Vector.__new__(d2.Vector))
+
