@@ -541,11 +541,24 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
     colrow = p.cols + int64_t(t.comp) * BS * p.nnz_node + int64_t(BS) * ra + e * L;
   }
   const RowFix<D> F = load_row_fix_n<D, P, FP1, NFIX>(p, node);
-  // the row node is relabelled local node 0 (vertex) or K-1 (edge (0,1));
-  // its column is the same for every incidence: accumulate it in a register
+  // The unit owns acc[my, my + L) alone (the units' segments partition the
+  // tile's), so it clears its own segment: no block barrier before the row
+  // walk, whose first loads are already in flight.
+  for (int32_t k = 0; k < L; ++k) my[k] = 0.0;
+  // The row node is relabelled local node 0 (vertex) or K-1 (edge (0,1)),
+  // and an edge's end vertices are local nodes 0 and 1: these NREG columns
+  // are the same for every incidence, so they are summed in registers (in
+  // incidence order, as the segment would) and added once at the end.
+  constexpr int NREG = vertex ? 1 : 3;
   constexpr int jstar = vertex ? 0 : E::K - 1;
-  double diag = 0.0;
-  uint32_t dslot = 0;
+  auto regcol = [](int i) { return i == 0 ? jstar : i - 1; };
+  double rsum[NREG];
+  uint32_t rslot[NREG];
+#pragma unroll
+  for (int i = 0; i < NREG; ++i) {
+    rsum[i] = 0.0;
+    rslot[i] = 0;
+  }
   // the next record is fetched one incidence ahead: its load (the head of
   // the dependent chain record -> vertex records -> geometry) overlaps the
   // current incidence's arithmetic
@@ -581,14 +594,23 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
         }
       }
     }
-    dslot = r.slot(jstar);
+#pragma unroll
+    for (int i = 0; i < NREG; ++i) {
+      rslot[i] = r.slot(regcol(i));
+      rsum[i] += double(out[regcol(i)]);
+    }
 #pragma unroll
     for (int j = 0; j < E::K; ++j) {
-      if (j == jstar) diag += double(out[j]);
-      else my[r.slot(j)] += double(out[j]);
+      bool in_reg = false;
+#pragma unroll
+      for (int i = 0; i < NREG; ++i) in_reg = in_reg || j == regcol(i);
+      if (!in_reg) my[r.slot(j)] += double(out[j]);
     }
   }
-  if (cnt) my[dslot] += diag;
+  if (cnt) {
+#pragma unroll
+    for (int i = 0; i < NREG; ++i) my[rslot[i]] += rsum[i];
+  }
   bpart[u] = bsum;
 }
 
@@ -607,8 +629,6 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
   const int32_t r0 = __ldg(p.node_rowptr + t.n0), r1 = __ldg(p.node_rowptr + t.n1);
   const int seg = BS * (r1 - r0);
   double* bpart = acc + seg;
-  for (int i = threadIdx.x; i < seg; i += blockDim.x) acc[i] = 0.0;
-  __syncthreads();
   const int units = (t.n1 - t.n0) * BS;
   if (int(threadIdx.x) < units) {
     // tiles never mix vertex and edge nodes (the host cuts P2 tiles at the
