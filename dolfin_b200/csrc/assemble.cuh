@@ -658,25 +658,22 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
   __syncthreads();
 }
 
-// Resident 256-thread blocks per SM that the launch bounds guarantee, which
-// caps registers per thread (65536 / (256 x blocks)).  The kernel is latency
-// bound, so warps per SM matter, but the P2 rows keep up to 15 kappa
-// combinations and W' entries live across their FMA chains; measured on
-// B200, two blocks (128 registers) beat three (85 registers, with spills):
-// P2 tets n=96 1.71 ms against 1.83 ms, vector P2 elasticity n=48 1.56 ms
-// against 1.83 ms, P1 tets n=32 0.041 ms against 0.045 ms.
-#ifndef DB2_TILE_MIN_BLOCKS_P1
-#define DB2_TILE_MIN_BLOCKS_P1 2
+// Register cap of the tile kernel (threads per CTA are chosen per pattern,
+// 32..256, so the cap is given directly rather than through launch bounds).
+// The kernel is latency bound, so resident warps per SM matter: with 64-thread
+// tiles, 96 registers give 10 CTAs per SM against 8 at the ~120 the P2 rows
+// take uncapped.  Measured on B200 (ms per A+b step): vector P2 elasticity
+// n=48 1.346 against 1.373 (uncapped within 128), P2 tets n=96 1.304 against
+// 1.325, P1 tets n=96 0.237 against 0.265; 104 registers was slower on the P2
+// rows, 88 no faster, 80 spills.
+#ifndef DB2_TILE_MAXNREG_P1
+#define DB2_TILE_MAXNREG_P1 96
 #endif
-#ifndef DB2_TILE_MIN_BLOCKS_P2
-#define DB2_TILE_MIN_BLOCKS_P2 2
+#ifndef DB2_TILE_MAXNREG_P2
+#define DB2_TILE_MAXNREG_P2 96
 #endif
-template <int P>
-constexpr int tile_min_blocks() {
-  return P == 1 ? DB2_TILE_MIN_BLOCKS_P1 : DB2_TILE_MIN_BLOCKS_P2;
-}
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
-__global__ void __launch_bounds__(kMaxTileThreads, tile_min_blocks<P>()) k_assemble(const AsmParams p) {
+__global__ void __maxnreg__(P == 1 ? DB2_TILE_MAXNREG_P1 : DB2_TILE_MAXNREG_P2) k_assemble(const AsmParams p) {
   extern __shared__ double acc[];
   tile_body<D, P, FORM, KP1, LOADM, CT>(p, p.tiles[blockIdx.x], acc);
 }
