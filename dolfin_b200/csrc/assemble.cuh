@@ -665,15 +665,24 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
 // take uncapped.  Measured on B200 (ms per A+b step): vector P2 elasticity
 // n=48 1.346 against 1.373 (uncapped within 128), P2 tets n=96 1.304 against
 // 1.325, P1 tets n=96 0.237 against 0.265; 104 registers was slower on the P2
-// rows, 88 no faster, 80 spills.
+// rows, 88 no faster, 80 spills.  The FP32-contraction rows keep fewer
+// values live and take 80 (12 CTAs): 1.03-1.05x their time at 96 on the
+// elasticity and P1 workloads, no change on P2 n=96.
 #ifndef DB2_TILE_MAXNREG_P1
 #define DB2_TILE_MAXNREG_P1 96
 #endif
 #ifndef DB2_TILE_MAXNREG_P2
 #define DB2_TILE_MAXNREG_P2 96
 #endif
+#ifndef DB2_TILE_MAXNREG_F32
+#define DB2_TILE_MAXNREG_F32 80
+#endif
+template <int P, typename CT>
+constexpr int tile_maxnreg() {
+  return sizeof(CT) == 4 ? DB2_TILE_MAXNREG_F32 : P == 1 ? DB2_TILE_MAXNREG_P1 : DB2_TILE_MAXNREG_P2;
+}
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
-__global__ void __maxnreg__(P == 1 ? DB2_TILE_MAXNREG_P1 : DB2_TILE_MAXNREG_P2) k_assemble(const AsmParams p) {
+__global__ void __maxnreg__((tile_maxnreg<P, CT>())) k_assemble(const AsmParams p) {
   extern __shared__ double acc[];
   tile_body<D, P, FORM, KP1, LOADM, CT>(p, p.tiles[blockIdx.x], acc);
 }
