@@ -24,6 +24,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "generated/element_rows.h"
 #include "internal.h"
 
@@ -236,6 +238,7 @@ struct AsmParams {
   const uint32_t* inc;       // node-contiguous incidence words (cell | local node << 28)
   const unsigned char* rec;  // interleaved incidence records (El::RS bytes each)
   const uint32_t* rec_goff;  // first record of each block of 32 nodes
+  const unsigned char* rec_first;  // record of each node's first incidence, by node
   const uint32_t* cells;
   const uint32_t* edge_v;    // P2: sorted endpoints of each edge node
   const double* xw;          // vertex records: 3D (x,y,z,kappa), 2D (x,y,kappa,f)
@@ -277,16 +280,21 @@ __device__ __forceinline__ uint32_t rec_index(const AsmParams& p, uint32_t node,
 }
 
 template <int D, int P>
-__device__ __forceinline__ Rec<D, P> load_rec(const AsmParams& p, uint32_t idx) {
+__device__ __forceinline__ Rec<D, P> load_rec_from(const unsigned char* base, uint32_t idx) {
   Rec<D, P> r;
   if constexpr (El<D, P>::RS == 16) {
-    const uint4 v = __ldg(reinterpret_cast<const uint4*>(p.rec) + idx);
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(base) + idx);
     r.w[0] = v.x; r.w[1] = v.y; r.w[2] = v.z; r.w[3] = v.w;
   } else {
-    const uint2 v = __ldg(reinterpret_cast<const uint2*>(p.rec) + idx);
+    const uint2 v = __ldg(reinterpret_cast<const uint2*>(base) + idx);
     r.w[0] = v.x; r.w[1] = v.y;
   }
   return r;
+}
+
+template <int D, int P>
+__device__ __forceinline__ Rec<D, P> load_rec(const AsmParams& p, uint32_t idx) {
+  return load_rec_from<D, P>(p.rec, idx);
 }
 
 // Relabelled vertex ids of a cell for local node li (vertex ids v[] as stored).
@@ -407,6 +415,34 @@ __device__ __forceinline__ void record_cell_n(const AsmParams& p, const RowFix<D
       const uint32_t v = uint32_t(int32_t(F.base) + r.delta(a - NFIX));
       load_vertex<D, FP1>(p, v, x[a], kap[a], fv[a]);
     }
+  }
+}
+
+// Fixed vertices by id only: their records are loaded again with each
+// incidence (L1 hits), so no coordinates stay live across the row walk.
+struct RowFixId {
+  uint32_t v[2];
+};
+template <int D, int P, int NFIX>
+__device__ __forceinline__ RowFixId load_row_fix_id(const AsmParams& p, uint32_t node) {
+  RowFixId r;
+  if constexpr (NFIX == 1) {
+    r.v[0] = r.v[1] = node;
+  } else {
+    const uint2 e = __ldg(reinterpret_cast<const uint2*>(p.edge_v) + (node - p.nverts));
+    r.v[0] = e.x;
+    r.v[1] = e.y;
+  }
+  return r;
+}
+template <int D, int P, bool FP1, int NFIX>
+__device__ __forceinline__ void record_cell_id(const AsmParams& p, const RowFixId& F,
+                                               const Rec<D, P>& r, double (&x)[D + 1][D],
+                                               double (&kap)[D + 1], double (&fv)[D + 1]) {
+#pragma unroll
+  for (int a = 0; a <= D; ++a) {
+    const uint32_t v = a < NFIX ? F.v[a] : uint32_t(int32_t(F.v[0]) + r.delta(a - NFIX));
+    load_vertex<D, FP1>(p, v, x[a], kap[a], fv[a]);
   }
 }
 
@@ -540,7 +576,15 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
     row_g = row_bc ? __ldg(p.bc_vals + rowdof) : 0.0;
     colrow = p.cols + int64_t(t.comp) * BS * p.nnz_node + int64_t(BS) * ra + e * L;
   }
-  const RowFix<D> F = load_row_fix_n<D, P, FP1, NFIX>(p, node);
+  // Elasticity rows reload their fixed vertices with every incidence (L1
+  // hits) and run at a lower register cap; the Poisson rows keep them in
+  // registers (measured on B200: reloading costs 10 % on P2 Poisson, gains
+  // 2 % on elasticity at 80 registers).
+  constexpr bool RELOAD = FORM == FORM_ELAS;
+  using Fix = typename std::conditional<RELOAD, RowFixId, RowFix<D>>::type;
+  Fix F;
+  if constexpr (RELOAD) F = load_row_fix_id<D, P, NFIX>(p, node);
+  else F = load_row_fix_n<D, P, FP1, NFIX>(p, node);
   // The unit owns acc[my, my + L) alone (the units' segments partition the
   // tile's), so it clears its own segment: no block barrier before the row
   // walk, whose first loads are already in flight.
@@ -561,14 +605,16 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
   }
   // the next record is fetched one incidence ahead: its load (the head of
   // the dependent chain record -> vertex records -> geometry) overlaps the
-  // current incidence's arithmetic
+  // current incidence's arithmetic.  The first comes from the node-indexed
+  // copy, so it is issued beside the row's other loads, not after rec_goff.
   Rec<D, P> rn{};
-  if (cnt > 0) rn = load_rec<D, P>(p, rbase);
+  if (cnt > 0) rn = load_rec_from<D, P>(p.rec_first, node);
   for (uint32_t m = 0; m < cnt; ++m) {
     const Rec<D, P> r = rn;
     if (m + 1 < cnt) rn = load_rec<D, P>(p, rbase + 32u * (m + 1));
     double x[D + 1][D], kap[D + 1], fv[D + 1];
-    record_cell_n<D, P, FP1, NFIX>(p, F, r, x, kap, fv);
+    if constexpr (RELOAD) record_cell_id<D, P, FP1, NFIX>(p, F, r, x, kap, fv);
+    else record_cell_n<D, P, FP1, NFIX>(p, F, r, x, kap, fv);
     Geometry<D> G;
     geometry(x, G);
     CT out[E::K];
@@ -677,12 +723,18 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
 #ifndef DB2_TILE_MAXNREG_F32
 #define DB2_TILE_MAXNREG_F32 80
 #endif
-template <int P, typename CT>
+#ifndef DB2_TILE_MAXNREG_ELAS
+#define DB2_TILE_MAXNREG_ELAS 80
+#endif
+template <int P, int FORM, typename CT>
 constexpr int tile_maxnreg() {
-  return sizeof(CT) == 4 ? DB2_TILE_MAXNREG_F32 : P == 1 ? DB2_TILE_MAXNREG_P1 : DB2_TILE_MAXNREG_P2;
+  return sizeof(CT) == 4       ? DB2_TILE_MAXNREG_F32
+         : FORM == FORM_ELAS ? DB2_TILE_MAXNREG_ELAS
+         : P == 1            ? DB2_TILE_MAXNREG_P1
+                             : DB2_TILE_MAXNREG_P2;
 }
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
-__global__ void __maxnreg__((tile_maxnreg<P, CT>())) k_assemble(const AsmParams p) {
+__global__ void __maxnreg__((tile_maxnreg<P, FORM, CT>())) k_assemble(const AsmParams p) {
   extern __shared__ double acc[];
   tile_body<D, P, FORM, KP1, LOADM, CT>(p, p.tiles[blockIdx.x], acc);
 }

@@ -673,6 +673,7 @@ void Pattern::ensure_device() {
       rec_goff[g + 1] = rec_goff[g] + 32 * mx;
     }
     std::vector<uint8_t> rec(size_t(rec_goff[ngrp]) * rs, 0);
+    std::vector<uint8_t> first(size_t(nn) * rs, 0);
     std::atomic<int64_t> bad{-1};
     parallel_for(nn, [&](int64_t b, int64_t e) {
       for (int64_t i = b; i < e; ++i) {
@@ -691,6 +692,7 @@ void Pattern::ensure_device() {
             std::memcpy(r + 2 * (a - nfix), &d16, 2);
           }
           std::memcpy(r + 2 * nd, &pos[size_t(s) * kp], size_t(K));
+          if (s == inc_ptr[i]) std::memcpy(&first[size_t(i) * rs], r, size_t(rs));
         }
       }
     });
@@ -699,6 +701,7 @@ void Pattern::ensure_device() {
            "renumber the mesh vertices for locality", (long long)bad.load());
     d_rec.upload(rec.data(), rec.size());
     d_rec_goff.upload(rec_goff.data(), rec_goff.size() * sizeof(uint32_t));
+    d_rec_first.upload(first.data(), first.size());
   }
   d_cell_inc.upload(cell_inc.data(), cell_inc.size() * sizeof(uint32_t));
   d_tiles.upload(tiles.data(), tiles.size() * sizeof(Tile));

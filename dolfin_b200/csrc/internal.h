@@ -144,6 +144,9 @@ struct Pattern {
   int rs = 8;
   std::vector<uint32_t> rec_goff;    // per 32-node block: first record index
   DeviceBuffer d_node_rowptr, d_inc_ptr, d_inc, d_rec, d_rec_goff, d_cell_inc, d_tiles, d_rowptr, d_cols;
+  // each node's first record again, node-indexed: the row walk's first
+  // record load needs no rec_goff lookup before it
+  DeviceBuffer d_rec_first;
   bool on_device = false;
   void ensure_device();      // first GPU use: upload the plan, expand the CSR
   // dof-level CSR on the host in the natural numbering (component expansion

@@ -69,6 +69,7 @@ dev::AsmParams make_params(const Pattern& P) {
   p.inc_ptr = P.d_inc_ptr.as<uint32_t>();
   p.rec = P.d_rec.as<unsigned char>();
   p.rec_goff = P.d_rec_goff.as<uint32_t>();
+  p.rec_first = P.d_rec_first.as<unsigned char>();
   p.inc = P.d_inc.as<uint32_t>();
   p.cols = P.d_cols.as<int32_t>();
   p.edge_v = P.V->d_edge_vertices.as<uint32_t>();
