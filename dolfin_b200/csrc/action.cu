@@ -1,5 +1,6 @@
-// action.cu -- matrix-free action y = A x and the adjoint (VJP) with respect
-// to a P1 coefficient, on the same row-gather plan as assembly.
+// action.cu -- matrix-free action y = A x (cell-wise element actions, then a
+// per-row gather in cell order) and the adjoint (VJP) with respect to a P1
+// coefficient.
 #include <cuda_runtime.h>
 
 #include "launch.cuh"
@@ -7,39 +8,221 @@
 namespace db2 {
 namespace dev {
 
-// y[(c,i)] = sum over cells K around node i of sum_{e,j} A^K_{(c,i),(e,j)} x[(e,j)]
-// (one thread per dof row, register accumulation in cell order; the x index
-// of column slot q of block e is the CSR column itself).
-template <int D, int P, int FORM, bool KP1, typename CT>
-__global__ void __launch_bounds__(256) k_apply(const AsmParams p, const double* __restrict__ xin,
-                                               double* __restrict__ y) {
-  using E = El<D, P>;
-  constexpr int BS = FORM == FORM_ELAS ? D : 1;
-  const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (r >= p.nnodes * BS) return;
-  const int c = int(r / p.nnodes);
-  const uint32_t node = uint32_t(r - int64_t(c) * p.nnodes);
-  const int32_t ra = __ldg(p.node_rowptr + node);
-  const int32_t L = __ldg(p.node_rowptr + node + 1) - ra;
-  const int32_t* crow = p.cols + int64_t(c) * BS * p.nnz_node + int64_t(BS) * ra;
-  const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - __ldg(p.inc_ptr + node);
-  const uint32_t rbase = __ldg(p.rec_goff + (node >> 5)) + (node & 31u);
-  const RowFix<D> F = load_row_fix<D, P, false>(p, node);
-  double acc = 0.0;
-  for (uint32_t m = 0; m < cnt; ++m) {
-    const Rec<D, P> rr = load_rec<D, P>(p, rbase + 32u * m);
-    double x[D + 1][D], kap[D + 1], fv[D + 1];
-    record_cell<D, P, false>(p, F, rr, x, kap, fv);
-    Geometry<D> G;
-    geometry(x, G);
-#pragma unroll 1
-    for (int e = 0; e < BS; ++e) {
-      CT out[E::K];
-      element_row<D, P, FORM, KP1, CT>(p, G, F.nfix == 1, c, e, kap, out);
+// Matrix-free action y = A x in two steps, without forming A.
+//
+// Step 1: the element action y_K = A_K x_K of every cell, by quadrature in
+// barycentric coordinates (sum factorisation of the element kernels: the
+// gradient of the trial function at a point, then its flux tested against
+// every basis function), written once per (cell, component, local node).
+// With lambda the barycentric coordinates and g_a = grad(lambda_a):
+//   P2 basis derivatives  dphi_v/dl_a = delta_va (4 l_v - 1),
+//                         dphi_(p,q)/dl_p = 4 l_q, dphi_(p,q)/dl_q = 4 l_p;
+//   grad u = sum_a U_a g_a,  U_a = sum_j x_j dphi_j/dl_a;
+//   y_j  += w |T| sum_a dphi_j/dl_a S_a,  S_a = flux . g_a,
+// where the flux is kappa grad u (diffusion) or the stress row
+// sigma_c = lambda div(u) e_c + mu (grad u + grad u^T)_c (elasticity; one
+// thread per output component c).  The rules integrate the element
+// integrands exactly: P1 -- the centroid (kappa linear, gradients
+// constant); P2 diffusion -- degree 3 (kappa linear times two linear
+// gradients); P2 elasticity -- degree 2.
+template <int D, int DEG>
+struct Quad;
+template <int D>
+struct Quad<D, 1> {  // centroid
+  static constexpr int NQ = 1;
+  __host__ __device__ static constexpr double w(int) { return 1.0; }
+  __host__ __device__ static constexpr double lam(int, int) { return 1.0 / (D + 1); }
+};
+// Hammer-Marlowe-Stroud tetrahedron rule of degree 2: (a, b, b, b) and
+// permutations, a = (5 + 3 sqrt 5) / 20, b = (5 - sqrt 5) / 20, weights 1/4.
+template <>
+struct Quad<3, 2> {
+  static constexpr int NQ = 4;
+  __host__ __device__ static constexpr double w(int) { return 0.25; }
+  __host__ __device__ static constexpr double lam(int q, int a) {
+    return a == q ? 0.5854101966249685 : 0.1381966011250105;
+  }
+};
+// Stroud's degree-3 rules: tetrahedron -4/5 at the centroid and 9/20 at
+// (1/2, 1/6, 1/6, 1/6) and permutations; triangle -27/48 at the centroid and
+// 25/48 at (3/5, 1/5, 1/5) and permutations.
+template <>
+struct Quad<3, 3> {
+  static constexpr int NQ = 5;
+  __host__ __device__ static constexpr double w(int q) { return q == 0 ? -0.8 : 0.45; }
+  __host__ __device__ static constexpr double lam(int q, int a) {
+    return q == 0 ? 0.25 : (a == q - 1 ? 0.5 : 1.0 / 6.0);
+  }
+};
+template <>
+struct Quad<2, 3> {
+  static constexpr int NQ = 4;
+  __host__ __device__ static constexpr double w(int q) { return q == 0 ? -27.0 / 48.0 : 25.0 / 48.0; }
+  __host__ __device__ static constexpr double lam(int q, int a) {
+    return q == 0 ? 1.0 / 3.0 : (a == q - 1 ? 0.6 : 0.2);
+  }
+};
+
+// grad(lambda_a) of the affine simplex and |T|.
+template <int D>
+__device__ __forceinline__ double bary_gradients(const double (&x)[D + 1][D], double (&g)[D + 1][D]) {
+  Geometry<D> G;
+  geometry(x, G);  // n[a] = det(J) grad(lambda_a), vol = |T|
+  double det;
+  if constexpr (D == 3) {
+    det = (x[1][0] - x[0][0]) * G.n[1][0] + (x[1][1] - x[0][1]) * G.n[1][1] + (x[1][2] - x[0][2]) * G.n[1][2];
+  } else {
+    det = (x[1][0] - x[0][0]) * G.n[1][0] + (x[1][1] - x[0][1]) * G.n[1][1];
+  }
+  // 1/det from the geometry's 1/(D! |det|)
+  const double inv = (D == 3 ? 6.0 : 2.0) * G.s * (det < 0.0 ? -1.0 : 1.0);
 #pragma unroll
-      for (int j = 0; j < E::K; ++j)
-        acc = fma(double(out[j]), __ldg(xin + __ldg(crow + e * L + rr.slot(j))), acc);
+  for (int a = 0; a <= D; ++a)
+#pragma unroll
+    for (int r = 0; r < D; ++r) g[a][r] = G.n[a][r] * inv;
+  return G.vol;
+}
+
+// U_a = sum_j x_j dphi_j/dl_a at barycentric point l, for one component.
+template <int D, int P, typename CT>
+__device__ __forceinline__ CT node_derivative(const CT (&xc)[El<D, P>::K], const double (&l)[D + 1], int a) {
+  constexpr int NB = D + 1;
+  if constexpr (P == 1) {
+    return xc[a];
+  } else {
+    CT u = CT(4.0 * l[a] - 1.0) * xc[a];
+#pragma unroll
+    for (int e = 0; e < El<D, P>::NE; ++e) {
+      const int p0 = edge_end(D, e, 0), p1 = edge_end(D, e, 1);
+      if (p0 == a) u = fma(CT(4.0 * l[p1]), xc[NB + e], u);
+      if (p1 == a) u = fma(CT(4.0 * l[p0]), xc[NB + e], u);
     }
+    return u;
+  }
+}
+
+// y_j += sum_a dphi_j/dl_a S_a at barycentric point l.
+template <int D, int P, typename CT>
+__device__ __forceinline__ void test_basis(const CT (&S)[D + 1], const double (&l)[D + 1],
+                                           double (&y)[El<D, P>::K]) {
+  constexpr int NB = D + 1;
+#pragma unroll
+  for (int v = 0; v < NB; ++v) y[v] += double(P == 1 ? S[v] : CT(4.0 * l[v] - 1.0) * S[v]);
+  if constexpr (P == 2) {
+#pragma unroll
+    for (int e = 0; e < El<D, P>::NE; ++e) {
+      const int p0 = edge_end(D, e, 0), p1 = edge_end(D, e, 1);
+      y[NB + e] += double(fma(CT(4.0 * l[p1]), S[p0], CT(4.0 * l[p0]) * S[p1]));
+    }
+  }
+}
+
+template <int D, int P, int FORM, bool KP1, typename CT>
+__global__ void __launch_bounds__(256) k_apply_cells(const AsmParams p, int64_t ncells,
+                                                     const double* __restrict__ xin,
+                                                     double* __restrict__ ycell) {
+  constexpr int NB = D + 1, K = El<D, P>::K;
+  constexpr bool ELAS = FORM == FORM_ELAS;
+  constexpr int BS = ELAS ? D : 1, n = BS * K;
+  using Q = Quad<D, P == 1 ? 1 : (ELAS ? 2 : 3)>;
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t cell = ELAS ? t / D : t;
+  const int c = ELAS ? int(t - cell * D) : 0;
+  if (cell >= ncells) return;
+  double xv[NB][D], kap[NB];
+#pragma unroll
+  for (int a = 0; a < NB; ++a) {
+    double f;
+    load_vertex<D, false>(p, __ldg(p.cells + size_t(cell) * NB + a), xv[a], kap[a], f);
+  }
+  double g[NB][D];
+  const double vol = bary_gradients<D>(xv, g);
+  CT gc[NB][D];
+#pragma unroll
+  for (int a = 0; a < NB; ++a)
+#pragma unroll
+    for (int r = 0; r < D; ++r) gc[a][r] = CT(g[a][r]);
+  CT xc[BS][K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const uint32_t node = __ldg(p.cell_nodes + size_t(cell) * K + j);
+#pragma unroll
+    for (int e = 0; e < BS; ++e) xc[e][j] = CT(__ldg(xin + int64_t(e) * p.nnodes + node));
+  }
+  double y[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) y[j] = 0.0;
+#pragma unroll
+  for (int q = 0; q < Q::NQ; ++q) {
+    double l[NB];
+#pragma unroll
+    for (int a = 0; a < NB; ++a) l[a] = Q::lam(q, a);
+    double wq = Q::w(q) * vol;
+    // grad u: gu[e][d] = sum_a U_a^e g_a[d]
+    CT gu[BS][D];
+#pragma unroll
+    for (int e = 0; e < BS; ++e) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) gu[e][d] = CT(0);
+#pragma unroll
+      for (int a = 0; a < NB; ++a) {
+        const CT u = node_derivative<D, P, CT>(xc[e], l, a);
+#pragma unroll
+        for (int d = 0; d < D; ++d) gu[e][d] = fma(u, gc[a][d], gu[e][d]);
+      }
+    }
+    CT flux[D];
+    if constexpr (ELAS) {
+      CT div = gu[0][0];
+#pragma unroll
+      for (int d = 1; d < D; ++d) div += gu[d][d];
+#pragma unroll
+      for (int d = 0; d < D; ++d) flux[d] = CT(p.mu) * (gu[c][d] + gu[d][c]);
+      flux[c] = fma(CT(p.lmbda), div, flux[c]);
+    } else {
+      double k = p.kscale;
+      if constexpr (KP1) {
+        double kq = 0.0;
+#pragma unroll
+        for (int a = 0; a < NB; ++a) kq = fma(kap[a], l[a], kq);
+        k *= kq;
+      }
+#pragma unroll
+      for (int d = 0; d < D; ++d) flux[d] = CT(k) * gu[0][d];
+    }
+    CT S[NB];
+#pragma unroll
+    for (int a = 0; a < NB; ++a) {
+      CT sa = flux[0] * gc[a][0];
+#pragma unroll
+      for (int d = 1; d < D; ++d) sa = fma(flux[d], gc[a][d], sa);
+      S[a] = CT(wq) * sa;
+    }
+    test_basis<D, P, CT>(S, l, y);
+  }
+#pragma unroll
+  for (int j = 0; j < K; ++j) ycell[size_t(cell) * n + c * K + j] = y[j];
+}
+
+// Step 2 (one thread per dof row (c, node)): y = sum of the element actions
+// of the node's incident cells, in ascending cell order -- a fixed order, so
+// the result is bitwise repeatable.
+template <int BS, int K>
+__global__ void __launch_bounds__(256) k_apply_gather(const uint32_t* __restrict__ inc_ptr,
+                                                      const uint32_t* __restrict__ inc,
+                                                      int64_t nnodes, const double* __restrict__ ycell,
+                                                      double* __restrict__ y) {
+  constexpr int n = BS * K;
+  const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= nnodes * BS) return;
+  const int c = int(r / nnodes);
+  const int64_t node = r - int64_t(c) * nnodes;
+  const uint32_t s0 = __ldg(inc_ptr + node), s1 = __ldg(inc_ptr + node + 1);
+  double acc = 0.0;
+  for (uint32_t s = s0; s < s1; ++s) {
+    const uint32_t w = __ldg(inc + s);
+    const uint32_t cell = w & 0x0fffffffu, li = w >> 28;
+    acc += __ldg(ycell + size_t(cell) * n + c * K + li);
   }
   y[r] = acc;
 }
@@ -136,11 +319,22 @@ __global__ void __launch_bounds__(256) k_vjp_vertices(const AsmParams p, int64_t
 }
 
 template <int D, int P, int FORM, bool KP1, typename CT>
-void run_apply(const AsmParams& p, int bs, const double* x, double* y, cudaStream_t s) {
-  const int64_t n = p.nnodes * bs;
-  k_apply<D, P, FORM, KP1, CT><<<unsigned((n + 255) / 256), 256, 0, s>>>(p, x, y);
+void run_apply(const Pattern& Pt, const AsmParams& p, const double* x, double* y, cudaStream_t s) {
+  constexpr int K = El<D, P>::K, BS = FORM == FORM_ELAS ? D : 1, n = BS * K;
+  const int64_t nc = Pt.V->mesh->nc;
+  const size_t need = size_t(nc) * n * sizeof(double);
+  if (Pt.d_cellvals.bytes < need) Pt.d_cellvals.alloc(need);
+  double* ycell = Pt.d_cellvals.as<double>();
+  const int64_t threads = nc * (FORM == FORM_ELAS ? D : 1);
+  if (threads > 0) {
+    k_apply_cells<D, P, FORM, KP1, CT><<<unsigned((threads + 255) / 256), 256, 0, s>>>(p, nc, x, ycell);
+    count_launch();
+    check_cuda("apply launch");
+  }
+  const int64_t rows = p.nnodes * BS;
+  k_apply_gather<BS, K><<<unsigned((rows + 255) / 256), 256, 0, s>>>(p.inc_ptr, p.inc, p.nnodes, ycell, y);
   count_launch();
-  check_cuda("apply launch");
+  check_cuda("apply gather launch");
 }
 
 }  // namespace dev
@@ -166,11 +360,11 @@ void launch_apply(const Pattern& P, const FormArgs& a, int precision, const doub
 #define DB2_AP(D_, P_)                                                                  \
   if (D == D_ && deg == P_) {                                                           \
     if (kp1) {                                                                          \
-      if (fp32) dev::run_apply<D_, P_, dev::FORM_DIFF, true, float>(p, 1, x, y, s);     \
-      else dev::run_apply<D_, P_, dev::FORM_DIFF, true, double>(p, 1, x, y, s);         \
+      if (fp32) dev::run_apply<D_, P_, dev::FORM_DIFF, true, float>(P, p, x, y, s);     \
+      else dev::run_apply<D_, P_, dev::FORM_DIFF, true, double>(P, p, x, y, s);         \
     } else {                                                                            \
-      if (fp32) dev::run_apply<D_, P_, dev::FORM_DIFF, false, float>(p, 1, x, y, s);    \
-      else dev::run_apply<D_, P_, dev::FORM_DIFF, false, double>(p, 1, x, y, s);        \
+      if (fp32) dev::run_apply<D_, P_, dev::FORM_DIFF, false, float>(P, p, x, y, s);    \
+      else dev::run_apply<D_, P_, dev::FORM_DIFF, false, double>(P, p, x, y, s);        \
     }                                                                                   \
     return;                                                                             \
   }
@@ -181,11 +375,11 @@ void launch_apply(const Pattern& P, const FormArgs& a, int precision, const doub
     p.mu = a.f.mu;
     p.lmbda = a.f.lmbda;
     if (deg == 1) {
-      if (fp32) dev::run_apply<3, 1, dev::FORM_ELAS, false, float>(p, 3, x, y, s);
-      else dev::run_apply<3, 1, dev::FORM_ELAS, false, double>(p, 3, x, y, s);
+      if (fp32) dev::run_apply<3, 1, dev::FORM_ELAS, false, float>(P, p, x, y, s);
+      else dev::run_apply<3, 1, dev::FORM_ELAS, false, double>(P, p, x, y, s);
     } else {
-      if (fp32) dev::run_apply<3, 2, dev::FORM_ELAS, false, float>(p, 3, x, y, s);
-      else dev::run_apply<3, 2, dev::FORM_ELAS, false, double>(p, 3, x, y, s);
+      if (fp32) dev::run_apply<3, 2, dev::FORM_ELAS, false, float>(P, p, x, y, s);
+      else dev::run_apply<3, 2, dev::FORM_ELAS, false, double>(P, p, x, y, s);
     }
     return;
   }

@@ -99,6 +99,39 @@ __device__ __forceinline__ uint32_t perm_of(int li) {
   const uint64_t w = li < 8 ? (lo >> (8 * li)) : (hi >> (8 * (li - 8)));
   return uint32_t(w) & 0xffu;
 }
+// Relabelled local node j -> original local node for canonical node li,
+// packed 4 bits per node (the device form of db2::canonical_node_map).
+__host__ __device__ constexpr int cell_edge_of(int D, int a, int b) {
+  for (int e = 0; e < (D == 3 ? 6 : 3); ++e) {
+    const int p = edge_end(D, e, 0), q = edge_end(D, e, 1);
+    if ((p == a && q == b) || (p == b && q == a)) return e;
+  }
+  return -1;
+}
+__host__ __device__ constexpr uint64_t node_map_code(int D, int P, int li) {
+  const uint32_t pc = perm_code(D, li);
+  int perm[4] = {0, 0, 0, 0};
+  for (int a = 0; a <= D; ++a) perm[a] = int((pc >> (2 * a)) & 3u);
+  const int nb = D + 1, ne = P == 2 ? (D == 3 ? 6 : 3) : 0;
+  uint64_t code = 0;
+  for (int j = 0; j < nb + ne; ++j) {
+    const int o = j < nb ? perm[j]
+                         : nb + cell_edge_of(D, perm[edge_end(D, j - nb, 0)], perm[edge_end(D, j - nb, 1)]);
+    code |= uint64_t(o) << (4 * j);
+  }
+  return code;
+}
+// the code of a runtime li, by selection (no table in memory)
+template <int D, int P>
+__device__ __forceinline__ uint64_t node_map_of(int li) {
+  constexpr int K = P == 1 ? D + 1 : (D == 3 ? 10 : 6);
+  uint64_t m = node_map_code(D, P, 0);
+#pragma unroll
+  for (int q = 1; q < K; ++q)
+    if (li == q) m = node_map_code(D, P, q);
+  return m;
+}
+
 template <typename T>
 __device__ __forceinline__ T sel4(const T (&v)[4], uint32_t idx) {
   return idx == 0 ? v[0] : idx == 1 ? v[1] : idx == 2 ? v[2] : v[3];
@@ -228,6 +261,22 @@ DB2_ROWS_EDGE(2, p2tri, 6)
 };
 #undef DB2_ROWS
 #undef DB2_ROWS_EDGE
+
+// Relabelled local node j -> original local node, per canonical node li
+// (the cell-wise kernels: assemble_local and the matrix-free action).
+struct LocalMaps {
+  uint8_t map[10][10];
+};
+inline LocalMaps local_maps(int D, int deg) {
+  LocalMaps M{};
+  const int K = deg == 1 ? D + 1 : (D == 3 ? 10 : 6);
+  int map[10];
+  for (int li = 0; li < K; ++li) {
+    canonical_node_map(D, deg, li, map);
+    for (int j = 0; j < K; ++j) M.map[li][j] = uint8_t(map[j]);
+  }
+  return M;
+}
 
 // ---- kernel parameters ------------------------------------------------------
 struct AsmParams {

@@ -147,6 +147,9 @@ struct Pattern {
   // each node's first record again, node-indexed: the row walk's first
   // record load needs no rec_goff lookup before it
   DeviceBuffer d_rec_first;
+  // matrix-free action: per-cell element actions (cells x bs x k), grown on
+  // first use
+  mutable DeviceBuffer d_cellvals;
   bool on_device = false;
   void ensure_device();      // first GPU use: upload the plan, expand the CSR
   // dof-level CSR on the host in the natural numbering (component expansion

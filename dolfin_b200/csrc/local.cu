@@ -17,11 +17,6 @@
 namespace db2 {
 namespace dev {
 
-// Relabelled local node j -> original local node, per canonical node li.
-struct LocalMaps {
-  uint8_t map[10][10];
-};
-
 // Per local facet fl and facet node t of a cell: the cell-local vertices of
 // the relabelled facet (the node canonical) and the cell-local node of each
 // relabelled facet node.
@@ -124,17 +119,6 @@ __global__ void __launch_bounds__(256) k_local_facets(
 }  // namespace dev
 
 namespace {
-
-dev::LocalMaps local_maps(int D, int deg) {
-  dev::LocalMaps M{};
-  const int K = deg == 1 ? D + 1 : (D == 3 ? 10 : 6);
-  int map[10];
-  for (int li = 0; li < K; ++li) {
-    canonical_node_map(D, deg, li, map);
-    for (int j = 0; j < K; ++j) M.map[li][j] = uint8_t(map[j]);
-  }
-  return M;
-}
 
 // Same canonical facet order and relabelling as the facet assembly plan.
 dev::FacetMaps facet_maps(int D, int deg) {
@@ -256,7 +240,7 @@ void launch_local(Space& V, const FormArgs* a, const FormArgs* a_ds, int64_t nce
         break;
       default: fail(DB2_ERR_UNSUPPORTED, "form kind %d has no cell integral", a->f.kind);
     }
-    const dev::LocalMaps M = local_maps(D, deg);
+    const dev::LocalMaps M = dev::local_maps(D, deg);
     const int64_t nth = ncells * n;
     const unsigned grid = unsigned((nth + 255) / 256);
 #define DB2_LC(D_, P_, F_, K_, L_) \
