@@ -123,17 +123,19 @@ __global__ void __launch_bounds__(256) k_apply_cells(const AsmParams p, int64_t 
                                                      double* __restrict__ ycell) {
   constexpr int NB = D + 1, K = El<D, P>::K;
   constexpr bool ELAS = FORM == FORM_ELAS;
-  constexpr int BS = ELAS ? D : 1, n = BS * K;
+  constexpr int BS = ELAS ? D : 1;
   using Q = Quad<D, P == 1 ? 1 : (ELAS ? 2 : 3)>;
   const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t cell = ELAS ? t / D : t;
   const int c = ELAS ? int(t - cell * D) : 0;
   if (cell >= ncells) return;
   double xv[NB][D], kap[NB];
+  uint32_t vid[NB];
 #pragma unroll
   for (int a = 0; a < NB; ++a) {
     double f;
-    load_vertex<D, false>(p, __ldg(p.cells + size_t(cell) * NB + a), xv[a], kap[a], f);
+    vid[a] = __ldg(p.cells + size_t(cell) * NB + a);
+    load_vertex<D, false>(p, vid[a], xv[a], kap[a], f);
   }
   double g[NB][D];
   const double vol = bary_gradients<D>(xv, g);
@@ -145,7 +147,8 @@ __global__ void __launch_bounds__(256) k_apply_cells(const AsmParams p, int64_t 
   CT xc[BS][K];
 #pragma unroll
   for (int j = 0; j < K; ++j) {
-    const uint32_t node = __ldg(p.cell_nodes + size_t(cell) * K + j);
+    // vertex nodes are numbered as the vertices (natural numbering)
+    const uint32_t node = j < NB ? vid[j] : __ldg(p.cell_nodes + size_t(cell) * K + j);
 #pragma unroll
     for (int e = 0; e < BS; ++e) xc[e][j] = CT(__ldg(xin + int64_t(e) * p.nnodes + node));
   }
@@ -200,29 +203,44 @@ __global__ void __launch_bounds__(256) k_apply_cells(const AsmParams p, int64_t 
     }
     test_basis<D, P, CT>(S, l, y);
   }
+  if constexpr (ELAS) {
+    // cell-major (cell, c, j): the three component threads of a cell write
+    // one contiguous block
 #pragma unroll
-  for (int j = 0; j < K; ++j) ycell[size_t(cell) * n + c * K + j] = y[j];
+    for (int j = 0; j < K; ++j) ycell[(size_t(cell) * BS + c) * K + j] = y[j];
+  } else {
+    // each value goes to its incidence slot (node-contiguous, ascending cell
+    // order), so that step 2 reads every row's terms contiguously
+#pragma unroll
+    for (int j = 0; j < K; ++j) ycell[__ldg(p.cell_inc + size_t(cell) * K + j)] = y[j];
+  }
 }
 
 // Step 2 (one thread per dof row (c, node)): y = sum of the element actions
 // of the node's incident cells, in ascending cell order -- a fixed order, so
-// the result is bitwise repeatable.
-template <int BS, int K>
+// the result is bitwise repeatable.  Scalar forms read the terms contiguously
+// (incidence order); elasticity finds them through the incidence words
+// (cell | local node << 28) in the cell-major array, which measured faster
+// for its three component threads per cell (0.33 ms against 0.46 ms per
+// action, vector P2 on UnitCubeMesh(48)).
+template <int BS, int K, bool INC>
 __global__ void __launch_bounds__(256) k_apply_gather(const uint32_t* __restrict__ inc_ptr,
                                                       const uint32_t* __restrict__ inc,
                                                       int64_t nnodes, const double* __restrict__ ycell,
                                                       double* __restrict__ y) {
-  constexpr int n = BS * K;
   const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= nnodes * BS) return;
   const int c = int(r / nnodes);
   const int64_t node = r - int64_t(c) * nnodes;
   const uint32_t s0 = __ldg(inc_ptr + node), s1 = __ldg(inc_ptr + node + 1);
   double acc = 0.0;
-  for (uint32_t s = s0; s < s1; ++s) {
-    const uint32_t w = __ldg(inc + s);
-    const uint32_t cell = w & 0x0fffffffu, li = w >> 28;
-    acc += __ldg(ycell + size_t(cell) * n + c * K + li);
+  if constexpr (INC) {
+    for (uint32_t s = s0; s < s1; ++s) acc += __ldg(ycell + s);
+  } else {
+    for (uint32_t s = s0; s < s1; ++s) {
+      const uint32_t w = __ldg(inc + s);
+      acc += __ldg(ycell + (size_t(w & 0x0fffffffu) * BS + c) * K + (w >> 28));
+    }
   }
   y[r] = acc;
 }
@@ -332,7 +350,8 @@ void run_apply(const Pattern& Pt, const AsmParams& p, const double* x, double* y
     check_cuda("apply launch");
   }
   const int64_t rows = p.nnodes * BS;
-  k_apply_gather<BS, K><<<unsigned((rows + 255) / 256), 256, 0, s>>>(p.inc_ptr, p.inc, p.nnodes, ycell, y);
+  k_apply_gather<BS, K, FORM != FORM_ELAS><<<unsigned((rows + 255) / 256), 256, 0, s>>>(
+      p.inc_ptr, p.inc, p.nnodes, ycell, y);
   count_launch();
   check_cuda("apply gather launch");
 }

@@ -262,20 +262,18 @@ DB2_ROWS_EDGE(2, p2tri, 6)
 #undef DB2_ROWS
 #undef DB2_ROWS_EDGE
 
-// Relabelled local node j -> original local node, per canonical node li
-// (the cell-wise kernels: assemble_local and the matrix-free action).
-struct LocalMaps {
-  uint8_t map[10][10];
-};
-inline LocalMaps local_maps(int D, int deg) {
-  LocalMaps M{};
+// The device node maps (node_map_code) agree with the host's canonical
+// relabelling (db2::canonical_node_map, which the assembly plan's slots
+// follow); checked on the host before a cell-wise launch.
+inline void check_node_maps(int D, int deg) {
   const int K = deg == 1 ? D + 1 : (D == 3 ? 10 : 6);
   int map[10];
   for (int li = 0; li < K; ++li) {
     canonical_node_map(D, deg, li, map);
-    for (int j = 0; j < K; ++j) M.map[li][j] = uint8_t(map[j]);
+    for (int j = 0; j < K; ++j)
+      if (int((node_map_code(D, deg, li) >> (4 * j)) & 15u) != map[j])
+        fail(DB2_ERR_UNSUPPORTED, "device node map disagrees with the host's (li %d, j %d)", li, j);
   }
-  return M;
 }
 
 // ---- kernel parameters ------------------------------------------------------

@@ -26,7 +26,7 @@ struct FacetMaps {
 };
 
 template <int D, int P, int FORM, bool KP1, int LOADM>
-__global__ void __launch_bounds__(256) k_local_cell(const AsmParams p, const LocalMaps M,
+__global__ void __launch_bounds__(256) k_local_cell(const AsmParams p,
                                                     const uint32_t* __restrict__ list,
                                                     int64_t nlist, int64_t nc, int rank,
                                                     double* __restrict__ out) {
@@ -58,12 +58,13 @@ __global__ void __launch_bounds__(256) k_local_cell(const AsmParams p, const Loc
   const bool vertex = li < NB;
   if (rank == 2) {
     double* row = out + (size_t(idx) * n + c * K + li) * n;
+    const uint64_t mc = node_map_of<D, P>(li);
 #pragma unroll 1
     for (int e = 0; e < BS; ++e) {
       double o[K];
       element_row<D, P, FORM, KP1, double>(p, G, vertex, c, e, kap, o);
 #pragma unroll
-      for (int j = 0; j < K; ++j) row[e * K + M.map[li][j]] = o[j];
+      for (int j = 0; j < K; ++j) row[e * K + int((mc >> (4 * j)) & 15u)] = o[j];
     }
   } else {
     out[size_t(idx) * n + c * K + li] = load_row<D, P, LOADM>(p, G, vertex, c, fv);
@@ -240,11 +241,11 @@ void launch_local(Space& V, const FormArgs* a, const FormArgs* a_ds, int64_t nce
         break;
       default: fail(DB2_ERR_UNSUPPORTED, "form kind %d has no cell integral", a->f.kind);
     }
-    const dev::LocalMaps M = dev::local_maps(D, deg);
+    dev::check_node_maps(D, deg);
     const int64_t nth = ncells * n;
     const unsigned grid = unsigned((nth + 255) / 256);
 #define DB2_LC(D_, P_, F_, K_, L_) \
-  dev::k_local_cell<D_, P_, F_, K_, L_><<<grid, 256, 0, s>>>(p, M, list, ncells, m.nc, rank, out)
+  dev::k_local_cell<D_, P_, F_, K_, L_><<<grid, 256, 0, s>>>(p, list, ncells, m.nc, rank, out)
 #define DB2_LC_DP(D_, P_)                                                                    \
   if (D == D_ && deg == P_) {                                                                \
     if (form == dev::FORM_ELAS) {                                                            \
