@@ -317,11 +317,13 @@ __global__ void __launch_bounds__(256) k_vjp_cells(const AsmParams p, int64_t nc
         if (a == orig) acc[a] += s;
     }
   }
-  for (int a = 0; a < NB; ++a) t[cell * NB + a] = acc[a];
+  // in vertex-incidence order (vertex nodes come first in the node-contiguous
+  // incidence array), so that step 2 reads each vertex's terms contiguously
+  for (int a = 0; a < NB; ++a) t[__ldg(p.cell_inc + size_t(cell) * E::K + a)] = acc[a];
 }
 
 // Adjoint, step 2 (one thread per vertex): dkappa[v] = sum over cells around
-// v, in cell order, of t[cell][local index of v].
+// v, in cell order, of their terms for v (contiguous: incidence order).
 template <int D, int P>
 __global__ void __launch_bounds__(256) k_vjp_vertices(const AsmParams p, int64_t nv,
                                                       const double* __restrict__ t,
@@ -329,10 +331,8 @@ __global__ void __launch_bounds__(256) k_vjp_vertices(const AsmParams p, int64_t
   const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   double s = 0.0;
-  for (uint32_t ii = __ldg(p.inc_ptr + v); ii < __ldg(p.inc_ptr + v + 1); ++ii) {
-    const uint32_t word = __ldg(p.inc + ii);
-    s += __ldg(t + size_t(word & 0x0fffffffu) * (D + 1) + (word >> 28));
-  }
+  const uint32_t s1 = __ldg(p.inc_ptr + v + 1);
+  for (uint32_t ii = __ldg(p.inc_ptr + v); ii < s1; ++ii) s += __ldg(t + ii);
   dk[v] = s;
 }
 
