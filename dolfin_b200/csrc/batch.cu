@@ -48,14 +48,15 @@ __device__ __forceinline__ void batch_tile(const BatchMember& m, const Tile& t, 
 }
 
 // Persistent: each CTA repeatedly takes the next tile from the work counter.
-// Three resident blocks per SM (85 registers): the batched members are 2D
-// meshes, whose rows need fewer registers; 0.95 ms against 1.21 ms at one
-// block for 512 triangle meshes.
-#ifndef DB2_BATCH_MIN_BLOCKS
-#define DB2_BATCH_MIN_BLOCKS 3
+// Register cap 64 (16 resident 64-thread CTAs per SM): the batched members
+// are 2D meshes, whose rows need fewer registers; measured on B200 for 512
+// triangle meshes (ms per graph replay): 0.770 at 64 registers against 0.788
+// at 72, 0.847 at 80 (some spills at 64 and 72, none at 96: 0.975).
+#ifndef DB2_BATCH_MAXNREG
+#define DB2_BATCH_MAXNREG 64
 #endif
 template <typename CT>
-__global__ void __launch_bounds__(kMaxTileThreads, DB2_BATCH_MIN_BLOCKS) k_batch(const BatchMember* __restrict__ members,
+__global__ void __maxnreg__(DB2_BATCH_MAXNREG) k_batch(const BatchMember* __restrict__ members,
                                                            const BatchTile* __restrict__ tiles,
                                                            int ntiles, unsigned int* counter) {
   extern __shared__ double acc[];
