@@ -1,9 +1,10 @@
 """Runs one named assembly workload a few times (for profiling with ncu).
 
-    python -m dolfin_b200.profile_case {elas|p2|p1} N [REPS]
+    python -m dolfin_b200.profile_case {elas|p2|p1} N [REPS] [action]
 
 elas: vector P2 elasticity on UnitCubeMesh(N) jittered 0.15h (A and b);
 p2 / p1: kappa*grad(u).grad(v) + f*v on P2 / P1 with P1 kappa, f.
+With "action" the matrix-free y = A x is run REPS times instead (x seeded).
 """
 import sys, os
 import torch, numpy as np
@@ -28,6 +29,15 @@ else:
     u, v = d2.TrialFunction(V), d2.TestFunction(V)
     a = kappa*d2.inner(d2.grad(u), d2.grad(v))*d2.dx
     L = f*v*d2.dx
+if len(sys.argv) > 4 and sys.argv[4] == "action":
+    x = torch.randn(V.dim(), dtype=torch.float64, device="cuda",
+                    generator=torch.Generator("cuda").manual_seed(3))
+    y = d2.Vector(torch.empty_like(x))
+    for _ in range(reps):
+        d2.assemble_action(a, d2.Vector(x), y)
+    torch.cuda.synchronize()
+    print(kind, n, "cells", mesh.num_cells(), "action |y|", float(y.tensor().norm()))
+    sys.exit(0)
 S = d2.SystemAssembler(a, L)
 A, b = d2.Matrix(), d2.Vector(n=V.dim())
 for _ in range(reps):
