@@ -204,10 +204,10 @@ __global__ void __launch_bounds__(256) k_apply_cells(const AsmParams p, int64_t 
     test_basis<D, P, CT>(S, l, y);
   }
   if constexpr (ELAS) {
-    // cell-major (cell, c, j): the three component threads of a cell write
-    // one contiguous block
+    // cell-major (cell, j, c): a node's three components of one cell are
+    // adjacent, and the cell's three component threads fill one block
 #pragma unroll
-    for (int j = 0; j < K; ++j) ycell[(size_t(cell) * BS + c) * K + j] = y[j];
+    for (int j = 0; j < K; ++j) ycell[(size_t(cell) * K + j) * BS + c] = y[j];
   } else {
     // each value goes to its incidence slot (node-contiguous, ascending cell
     // order), so that step 2 reads every row's terms contiguously
@@ -216,33 +216,38 @@ __global__ void __launch_bounds__(256) k_apply_cells(const AsmParams p, int64_t 
   }
 }
 
-// Step 2 (one thread per dof row (c, node)): y = sum of the element actions
-// of the node's incident cells, in ascending cell order -- a fixed order, so
-// the result is bitwise repeatable.  Scalar forms read the terms contiguously
-// (incidence order); elasticity finds them through the incidence words
-// (cell | local node << 28) in the cell-major array, which measured faster
-// for its three component threads per cell (0.33 ms against 0.46 ms per
-// action, vector P2 on UnitCubeMesh(48)).
+// Step 2: y = sum of the element actions of the node's incident cells, in
+// ascending cell order -- a fixed order, so the result is bitwise
+// repeatable.  Scalar forms (one thread per row) read the terms
+// contiguously (incidence order).  Elasticity (one thread per node, all
+// components) finds them through the incidence words (cell | local node <<
+// 28) in the cell-major array, the three components of a term adjacent --
+// measured faster than component planes in incidence order for its three
+// component threads per cell (0.33 ms against 0.46 ms per action, vector P2
+// on UnitCubeMesh(48)).
 template <int BS, int K, bool INC>
 __global__ void __launch_bounds__(256) k_apply_gather(const uint32_t* __restrict__ inc_ptr,
                                                       const uint32_t* __restrict__ inc,
                                                       int64_t nnodes, const double* __restrict__ ycell,
                                                       double* __restrict__ y) {
-  const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (r >= nnodes * BS) return;
-  const int c = int(r / nnodes);
-  const int64_t node = r - int64_t(c) * nnodes;
+  const int64_t node = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (node >= nnodes) return;
   const uint32_t s0 = __ldg(inc_ptr + node), s1 = __ldg(inc_ptr + node + 1);
-  double acc = 0.0;
+  double acc[BS];
+#pragma unroll
+  for (int c = 0; c < BS; ++c) acc[c] = 0.0;
   if constexpr (INC) {
-    for (uint32_t s = s0; s < s1; ++s) acc += __ldg(ycell + s);
+    for (uint32_t s = s0; s < s1; ++s) acc[0] += __ldg(ycell + s);
   } else {
     for (uint32_t s = s0; s < s1; ++s) {
       const uint32_t w = __ldg(inc + s);
-      acc += __ldg(ycell + (size_t(w & 0x0fffffffu) * BS + c) * K + (w >> 28));
+      const double* t = ycell + (size_t(w & 0x0fffffffu) * K + (w >> 28)) * BS;
+#pragma unroll
+      for (int c = 0; c < BS; ++c) acc[c] += __ldg(t + c);
     }
   }
-  y[r] = acc;
+#pragma unroll
+  for (int c = 0; c < BS; ++c) y[int64_t(c) * nnodes + node] = acc[c];
 }
 
 // Adjoint, step 1 (one thread per cell): t[cell][m] = sum_{i,j in cell}
@@ -349,8 +354,7 @@ void run_apply(const Pattern& Pt, const AsmParams& p, const double* x, double* y
     count_launch();
     check_cuda("apply launch");
   }
-  const int64_t rows = p.nnodes * BS;
-  k_apply_gather<BS, K, FORM != FORM_ELAS><<<unsigned((rows + 255) / 256), 256, 0, s>>>(
+  k_apply_gather<BS, K, FORM != FORM_ELAS><<<unsigned((p.nnodes + 255) / 256), 256, 0, s>>>(
       p.inc_ptr, p.inc, p.nnodes, ycell, y);
   count_launch();
   check_cuda("apply gather launch");

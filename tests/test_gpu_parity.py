@@ -174,13 +174,17 @@ def test_deterministic_bitwise(orc):
     assert np.array_equal(A1, A2)
 
 
-@pytest.mark.parametrize("tdim,deg,vs,n", [(3, 1, 1, 5), (3, 2, 1, 3), (3, 2, 3, 3), (2, 2, 1, 7)])
+@pytest.mark.parametrize("tdim,deg,vs,n", [(3, 1, 1, 5), (3, 2, 1, 3), (3, 2, 3, 3), (2, 2, 1, 7),
+                                            (2, 1, 1, 9), (3, 1, 3, 4), (3, 2, 0, 3), (2, 2, 0, 6)])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_matrix_free_action_matches_csr(orc, tdim, deg, vs, n, precision):
+    """vs = 0: scalar space with a constant coefficient."""
     case = Case(orc, tdim, n, jitter=0.1, seed=10)
-    V = d2.FunctionSpace(case.mesh, "Lagrange", deg, value_size=vs)
+    V = d2.FunctionSpace(case.mesh, "Lagrange", deg, value_size=max(vs, 1))
     u, v = d2.TrialFunction(V), d2.TestFunction(V)
-    if vs == 1:
+    if vs == 0:
+        a = d2.Constant(1.7) * d2.inner(d2.grad(u), d2.grad(v)) * d2.dx
+    elif vs == 1:
         W = d2.FunctionSpace(case.mesh, "Lagrange", 1)
         kappa = d2.Function(W, synthetic.uniform_field(case.om.nv, 0.5, 2.0, seed=11))
         a = kappa * d2.inner(d2.grad(u), d2.grad(v)) * d2.dx
@@ -193,6 +197,9 @@ def test_matrix_free_action_matches_csr(orc, tdim, deg, vs, n, precision):
     yref = A @ x.cpu().numpy()
     tol = FP64_TOL * 10 if precision == "fp64" else FP32_TOL * 10
     assert vec_err(y, yref) <= tol
+    # the per-row sums run in a fixed order: a second action is bitwise equal
+    y2 = d2.assemble_action(a, d2.Vector(x), precision=precision).get_local()
+    assert np.array_equal(y, y2)
 
 
 @pytest.mark.parametrize("tdim,deg", [(3, 1), (3, 2), (2, 2)])
