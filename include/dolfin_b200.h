@@ -239,7 +239,11 @@ int db2_assemble_facets_bc(db2_pattern P, const db2_form* a_ds, const double* wa
                            const db2_form* L_ds, const double* wL, const uint8_t* bc_flags,
                            const double* bc_vals, double* vals, double* b, void* stream);
 /* Matrix-free action y = A(a) x (device x[N], y[N]); replaces assembling A
-   and calling GenericMatrix::mult (dolfin/la/GenericMatrix.h). */
+   and calling GenericMatrix::mult (dolfin/la/GenericMatrix.h).  Computed
+   per cell (element actions, exact quadrature) and summed per row in cell
+   order, so repeated calls agree bitwise.  The first call on a pattern
+   allocates cells * bs * k doubles of device work space, kept by the
+   pattern; calls on one pattern that overlap on the GPU race on it. */
 int db2_apply(db2_pattern P, const db2_form* a, const double* w, int precision, const double* x,
               double* y, void* stream);
 /* Vector-Jacobian product of (A(kappa), b(kappa)) for a = kappa grad.grad
