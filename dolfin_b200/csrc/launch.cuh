@@ -34,21 +34,69 @@ void allow_dynamic_smem(Kernel kern, unsigned long long& done) {
   if (dev < 64) done |= 1ull << dev;
 }
 
+#ifndef DB2_CLASS_STREAMS
+#define DB2_CLASS_STREAMS 1
+#endif
+// Side streams of the calling thread on the current device, for running the
+// tile classes of one assembly concurrently (they write disjoint rows).
+struct SideStreams {
+  static constexpr int kMax = 16;
+  cudaStream_t s[kMax] = {};
+  cudaEvent_t done[kMax] = {};
+  cudaEvent_t fork = nullptr;
+  bool ready = false;
+};
+inline SideStreams& side_streams() {
+  thread_local SideStreams per_device[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  SideStreams& S = per_device[dev & 63];
+  if (!S.ready) {
+    for (int i = 0; i < SideStreams::kMax; ++i) {
+      cudaStreamCreateWithFlags(&S.s[i], cudaStreamNonBlocking);
+      cudaEventCreateWithFlags(&S.done[i], cudaEventDisableTiming);
+    }
+    cudaEventCreateWithFlags(&S.fork, cudaEventDisableTiming);
+    check_cuda("side streams");
+    S.ready = true;
+  }
+  return S;
+}
+
+// One launch per shared-memory class.  The classes write disjoint rows, so
+// they run on side streams forked from and joined back to the caller's
+// stream: the shared-memory-heavy vertex-row tiles (launched first) and the
+// register-heavy edge-row tiles then share the SMs instead of each running
+// alone below the SM's residency limits.
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
 void run_assemble(const AsmParams& p, const LaunchCfg& cfg) {
   auto kern = k_assemble<D, P, FORM, KP1, LOADM, CT>;
   static unsigned long long configured = 0;
   allow_dynamic_smem(kern, configured);
   const auto& cb = *cfg.class_begin;
-  for (size_t k = 0; k + 1 < cb.size(); ++k) {
+  const int ncls = int(cb.size()) - 1;
+  const bool fork = DB2_CLASS_STREAMS && ncls > 1 && ncls <= SideStreams::kMax;
+  SideStreams* S = fork ? &side_streams() : nullptr;
+  if (fork) cudaEventRecord(S->fork, cfg.stream);
+  int used = 0;
+  for (int k = ncls - 1; k >= 0; --k) {  // largest segments first
     const int n = cb[k + 1] - cb[k];
     if (n <= 0) continue;
     AsmParams q = p;
     q.tiles = p.tiles + cb[k];
     const size_t smem = size_t((*cfg.class_smem)[k]) + size_t(cfg.threads) * sizeof(double);
-    kern<<<n, cfg.threads, smem, cfg.stream>>>(q);
+    cudaStream_t st = cfg.stream;
+    if (fork) {
+      st = S->s[used];
+      cudaStreamWaitEvent(st, S->fork, 0);
+    }
+    kern<<<n, cfg.threads, smem, st>>>(q);
     count_launch();
+    if (fork) cudaEventRecord(S->done[used], st);
+    ++used;
   }
+  if (fork)
+    for (int i = 0; i < used; ++i) cudaStreamWaitEvent(cfg.stream, S->done[i], 0);
   check_cuda("assemble launch");
 }
 
