@@ -679,6 +679,10 @@ void Pattern::ensure_device() {
     std::atomic<int64_t> bad{-1};
     parallel_for(nn, [&](int64_t b, int64_t e) {
       for (int64_t i = b; i < e; ++i) {
+        // edge-node rows: which of the record's slots this incidence is the
+        // first to touch (in incidence order), in the record's otherwise
+        // unused last offset field -- the kernel stores there instead of adding
+        uint64_t seen[4] = {0, 0, 0, 0};
         for (uint32_t s = inc_ptr[i]; s < inc_ptr[i + 1]; ++s) {
           const uint32_t c = inc[s] & 0x0fffffffu, li = inc[s] >> 28;
           int perm[4];
@@ -694,6 +698,17 @@ void Pattern::ensure_device() {
             std::memcpy(r + 2 * (a - nfix), &d16, 2);
           }
           std::memcpy(r + 2 * nd, &pos[size_t(s) * kp], size_t(K));
+          if (nfix == 2) {
+            uint16_t fm = 0;
+            for (int j = 0; j < K; ++j) {
+              const uint8_t sl = pos[size_t(s) * kp + j];
+              if (!(seen[sl >> 6] >> (sl & 63) & 1u)) {
+                fm = uint16_t(fm | (1u << j));
+                seen[sl >> 6] |= uint64_t(1) << (sl & 63);
+              }
+            }
+            std::memcpy(r + 2 * (D - 1), &fm, 2);
+          }
           if (s == inc_ptr[i]) std::memcpy(&first[size_t(i) * rs], r, size_t(rs));
         }
       }
