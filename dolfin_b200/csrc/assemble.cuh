@@ -629,9 +629,9 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
     colrow = p.cols + int64_t(t.comp) * BS * p.nnz_node + int64_t(BS) * ra + e * L;
   }
   // Elasticity rows reload their fixed vertices with every incidence (L1
-  // hits) and run at a lower register cap; the Poisson rows keep them in
-  // registers (measured on B200: reloading costs 10 % on P2 Poisson, gains
-  // 2 % on elasticity at 80 registers).
+  // hits); the Poisson rows keep them in registers (measured on B200:
+  // reloading costs 10 % on P2 Poisson; elasticity with first-touch stores at
+  // 96 registers: 1.20 ms reloading against 1.32 keeping them).
   constexpr bool RELOAD = FORM == FORM_ELAS;
   using Fix = typename std::conditional<RELOAD, RowFixId, RowFix<D>>::type;
   Fix F;
@@ -640,12 +640,11 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
   // The unit owns acc[my, my + L) alone (the units' segments partition the
   // tile's), so it clears its own segment: no block barrier before the row
   // walk, whose first loads are already in flight.
-  // Edge-node rows of the diffusion forms need no clearing: every slot of
-  // the row is written first by a plain store, at the incidence the record
-  // marks as its first (fewer shared-memory loads: P2 tets n=96 1.13 ms
-  // against 1.23).  The elasticity rows keep the clear-and-add path: at
-  // their 80-register cap the mask costs spills (1.33 ms against 1.28).
-  constexpr bool FIRSTF = NFIX == 2 && FORM != FORM_ELAS;
+  // Edge-node rows need no clearing: every slot of the row is written first
+  // by a plain store, at the incidence the record marks as its first (fewer
+  // shared-memory loads: P2 tets n=96 1.13 ms against 1.23, vector P2
+  // elasticity n=48 1.20 against 1.28).
+  constexpr bool FIRSTF = NFIX == 2;
   if (!FIRSTF || cnt == 0)
     for (int32_t k = 0; k < L; ++k) my[k] = 0.0;
   // The row node is relabelled local node 0 (vertex) or K-1 (edge (0,1)),
@@ -779,7 +778,9 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
 // take uncapped.  Measured on B200 (ms per A+b step): vector P2 elasticity
 // n=48 1.346 against 1.373 (uncapped within 128), P2 tets n=96 1.304 against
 // 1.325, P1 tets n=96 0.237 against 0.265; 104 registers was slower on the P2
-// rows, 88 no faster, 80 spills.  The FP32-contraction rows keep fewer
+// rows, 88 no faster, 80 spills.  The elasticity rows (first-touch stores,
+// fixed vertices reloaded) take 96 too: 1.20 ms against 1.35 at 88.  The
+// FP32-contraction rows keep fewer
 // values live and take 80 (12 CTAs): 1.03-1.05x their time at 96 on the
 // elasticity and P1 workloads, no change on P2 n=96.
 #ifndef DB2_TILE_MAXNREG_P1
@@ -792,7 +793,7 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
 #define DB2_TILE_MAXNREG_F32 80
 #endif
 #ifndef DB2_TILE_MAXNREG_ELAS
-#define DB2_TILE_MAXNREG_ELAS 80
+#define DB2_TILE_MAXNREG_ELAS 96
 #endif
 template <int P, int FORM, typename CT>
 constexpr int tile_maxnreg() {
