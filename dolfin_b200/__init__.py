@@ -16,7 +16,7 @@ hand-written CUDA kernels reached through the C ABI in include/dolfin_b200.h.
 from . import _capi
 from .assembling import (SystemAssembler, assemble, assemble_action, assemble_local,
                          assemble_system)
-from .io import File
+from .io import File, XDMFFile
 from .bcs import DirichletBC
 from .cpp import (DofMap, FunctionSpace, Mesh, SparsityPattern, UnitCubeMesh, UnitSquareMesh,
                   VectorFunctionSpace, parameters)
@@ -26,7 +26,7 @@ from .ufl import (Identity, SpatialCoordinate, TestFunction, TrialFunction, div,
                   inner, nabla_grad, sym, tr, transpose)
 
 __all__ = [
-    "assemble", "assemble_system", "assemble_action", "assemble_local", "SystemAssembler", "File",
+    "assemble", "assemble_system", "assemble_action", "assemble_local", "SystemAssembler", "File", "XDMFFile",
     "Mesh", "UnitCubeMesh",
     "UnitSquareMesh", "FunctionSpace", "VectorFunctionSpace", "DofMap", "SparsityPattern",
     "parameters", "Function", "Constant", "Matrix", "Vector", "TestFunction", "TrialFunction",

@@ -55,9 +55,11 @@ class Mesh(_Handle):
 
     def __init__(self, coordinates=None, cells=None, _handle=None):
         if _handle is None and (isinstance(coordinates, (str, bytes)) or hasattr(coordinates, "__fspath__")):
-            # Mesh("mesh.xml"): DOLFIN XML (dolfin/io/XMLMesh.cpp)
+            # Mesh("mesh.xml"): DOLFIN XML (dolfin/io/XMLMesh.cpp);
+            # Mesh("mesh.xdmf"): XDMF with inline data (dolfin/io/XDMFFile.cpp)
             h = C.c_void_p()
-            call("db2_mesh_read_xml", os.fsencode(coordinates), C.byref(h))
+            name = os.fsencode(coordinates)
+            call("db2_mesh_read_xdmf" if name.endswith(b".xdmf") else "db2_mesh_read_xml", name, C.byref(h))
             _handle = h
         if _handle is None:
             x = np.ascontiguousarray(coordinates, np.float64)

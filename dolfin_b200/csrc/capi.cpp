@@ -172,6 +172,23 @@ int db2_mesh_write_xml(db2_mesh m, const char* path) {
   });
 }
 
+int db2_mesh_read_xdmf(const char* path, db2_mesh* out) {
+  return guard([&] {
+    need(path, "path");
+    need(out, "out");
+    *out = new db2_mesh_t{db2::read_mesh_xdmf(path)};
+  });
+}
+
+int db2_mesh_write_xdmf(db2_mesh m, const char* path, const double* values, int value_size,
+                        const char* name) {
+  return guard([&] {
+    need(m, "mesh");
+    need(path, "path");
+    db2::write_mesh_xdmf(*m->m, path, values, value_size, name);
+  });
+}
+
 int db2_vector_write_xml(const char* path, int64_t n, const double* x) {
   return guard([&] {
     need(path, "path");

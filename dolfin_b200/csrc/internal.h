@@ -182,6 +182,9 @@ void build_reordered_csr(Pattern& P);
 // DOLFIN XML files (io.cpp).
 std::shared_ptr<Mesh> read_mesh_xml(const char* path);
 void write_mesh_xml(const Mesh& m, const char* path);
+std::shared_ptr<Mesh> read_mesh_xdmf(const char* path);
+void write_mesh_xdmf(const Mesh& m, const char* path, const double* values, int value_size,
+                     const char* name);
 void write_vector_xml(const char* path, int64_t n, const double* x);
 int64_t read_vector_xml(const char* path, double* x, int64_t cap);  // x NULL: size only
 // Host-side facet plan of a pattern (no device work); Pattern::facet_plan()

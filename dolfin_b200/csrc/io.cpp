@@ -21,6 +21,7 @@
 #include <map>
 #include <sstream>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "internal.h"
@@ -31,6 +32,7 @@ namespace {
 struct Tag {
   std::string name;
   std::map<std::string, std::string> attr;
+  size_t body = 0;  // offset just past the start tag (element text begins)
 };
 
 // All element start tags of the document, in order ('<?', '<!' and end tags
@@ -66,6 +68,7 @@ std::vector<Tag> scan_tags(const std::string& s) {
       t.attr[key] = s.substr(p, ve - p);
       p = ve + 1;
     }
+    t.body = end + 1;
     tags.push_back(std::move(t));
     i = end + 1;
   }
@@ -195,6 +198,146 @@ void write_vector_xml(const char* path, int64_t n, const double* x) {
   for (int64_t i = 0; i < n; ++i)
     s += "      <element index=\"" + std::to_string(i) + "\" value=\"" + fmt17(x[i]) + "\" />\n";
   s += "    </array>\n  </vector>\n</dolfin>\n";
+  write_file(path, s);
+}
+
+// ---- XDMF (ASCII encoding) ---------------------------------------------------
+// XDMFFile::write(mesh, Encoding::ASCII) / XDMFFile::read(mesh)
+// (dolfin/io/XDMFFile.cpp:91-131 add_mesh :1140, add_topology_data :1788,
+// add_geometry_data :1831, add_data_item :1879, vtk_cell_type_str :3090):
+//   <Xdmf Version="3.0"> <Domain> <Grid Name="mesh" GridType="Uniform">
+//     <Topology NumberOfElements="nc" TopologyType="Tetrahedron|Triangle"
+//               NodesPerElement="d+1">
+//       <DataItem Dimensions="nc d+1" NumberType="UInt" Format="XML"> ... </DataItem>
+//     <Geometry GeometryType="XYZ|XY">
+//       <DataItem Dimensions="nv d" Format="XML"> ... </DataItem>
+// HDF5-backed items (Format="HDF") need HDF5, which this build does not
+// have; affine (first-order) simplices with gdim == tdim only.
+namespace {
+
+// The whitespace-separated numbers of the DataItem that follows tag `k`.
+const Tag& data_item_after(const std::vector<Tag>& tags, size_t k, const char* path) {
+  for (size_t j = k + 1; j < tags.size(); ++j)
+    if (tags[j].name == "DataItem") {
+      auto f = tags[j].attr.find("Format");
+      const std::string fmt = f == tags[j].attr.end() ? "XML" : f->second;
+      if (fmt != "XML")
+        fail(DB2_ERR_UNSUPPORTED, "%s: DataItem Format=\"%s\" (HDF5-backed XDMF needs HDF5; write the "
+             "file with ASCII encoding)", path, fmt.c_str());
+      return tags[j];
+    }
+  fail(DB2_ERR_ARGUMENT, "%s: <%s> has no DataItem", path, tags[k].name.c_str());
+}
+
+std::vector<int64_t> dims_of(const Tag& t, const char* path) {
+  std::vector<int64_t> d;
+  std::istringstream in(need_attr(t, "Dimensions"));
+  int64_t v;
+  while (in >> v) d.push_back(v);
+  if (d.size() != 2 || d[0] < 0 || d[1] <= 0) fail(DB2_ERR_ARGUMENT, "%s: bad DataItem Dimensions", path);
+  return d;
+}
+
+template <typename T>
+std::vector<T> numbers(const std::string& s, const Tag& t, size_t count, const char* path) {
+  const size_t end = s.find('<', t.body);
+  std::vector<T> v;
+  v.reserve(count);
+  const char* p = s.c_str() + t.body;
+  const char* stop = s.c_str() + (end == std::string::npos ? s.size() : end);
+  while (v.size() < count) {
+    while (p < stop && isspace((unsigned char)*p)) ++p;
+    if (p >= stop) break;
+    char* e = nullptr;
+    if constexpr (std::is_floating_point<T>::value) {
+      const double x = std::strtod(p, &e);
+      if (e == p) fail(DB2_ERR_ARGUMENT, "%s: bad number in DataItem", path);
+      v.push_back(T(x));
+    } else {
+      const long long x = std::strtoll(p, &e, 10);
+      if (e == p || x < 0) fail(DB2_ERR_ARGUMENT, "%s: bad index in DataItem", path);
+      v.push_back(T(x));
+    }
+    p = e;
+  }
+  if (v.size() != count) fail(DB2_ERR_SHAPE, "%s: DataItem holds %zu values, Dimensions say %zu", path, v.size(), count);
+  return v;
+}
+
+}  // namespace
+
+std::shared_ptr<Mesh> read_mesh_xdmf(const char* path) {
+  const std::string s = read_file(path);
+  const std::vector<Tag> tags = scan_tags(s);
+  size_t kt = tags.size(), kg = tags.size();
+  for (size_t k = 0; k < tags.size(); ++k) {
+    if (tags[k].name == "Topology" && kt == tags.size()) kt = k;
+    if (tags[k].name == "Geometry" && kg == tags.size()) kg = k;
+  }
+  if (kt == tags.size() || kg == tags.size()) fail(DB2_ERR_ARGUMENT, "%s: no <Topology> / <Geometry>", path);
+  std::string tt = need_attr(tags[kt], "TopologyType");
+  std::transform(tt.begin(), tt.end(), tt.begin(), [](unsigned char c) { return char(std::tolower(c)); });
+  const int tdim = tt == "tetrahedron" ? 3 : (tt == "triangle" ? 2 : 0);
+  if (!tdim) fail(DB2_ERR_UNSUPPORTED, "%s: TopologyType %s (Triangle/Tetrahedron provided)", path, tt.c_str());
+  const std::string gt = need_attr(tags[kg], "GeometryType");
+  const int gdim = gt == "XYZ" ? 3 : (gt == "XY" ? 2 : 0);
+  if (gdim != tdim) fail(DB2_ERR_UNSUPPORTED, "%s: GeometryType %s with a %d-D cell (gdim == tdim provided)", path, gt.c_str(), tdim);
+  const Tag& ti = data_item_after(tags, kt, path);
+  const Tag& gi = data_item_after(tags, kg, path);
+  const std::vector<int64_t> td = dims_of(ti, path), gd = dims_of(gi, path);
+  if (td[1] != tdim + 1 || gd[1] != gdim) fail(DB2_ERR_SHAPE, "%s: DataItem shapes do not match the cell type", path);
+  const int64_t nc = td[0], nv = gd[0];
+  std::vector<uint32_t> cells = numbers<uint32_t>(s, ti, size_t(nc) * (tdim + 1), path);
+  const std::vector<double> x = numbers<double>(s, gi, size_t(nv) * gdim, path);
+  for (int64_t c = 0; c < nc; ++c) {
+    for (int a = 0; a <= tdim; ++a)
+      if (int64_t(cells[c * (tdim + 1) + a]) >= nv)
+        fail(DB2_ERR_INDEX, "%s: cell %lld vertex %u", path, (long long)c, cells[c * (tdim + 1) + a]);
+    std::sort(cells.begin() + c * (tdim + 1), cells.begin() + (c + 1) * (tdim + 1));
+  }
+  return make_mesh(tdim, nv, x.data(), nc, cells.data());
+}
+
+// With values (nv x value_size, vertex order) a P1 field is added as a
+// node-centred Attribute, as XDMFFile::write(const Function&) does for a
+// vertex-based function (:311-397).
+void write_mesh_xdmf(const Mesh& m, const char* path, const double* values, int value_size,
+                     const char* name) {
+  if (values && value_size != 1 && value_size != m.tdim)
+    fail(DB2_ERR_SHAPE, "XDMF attribute: value size %d (1 or %d provided)", value_size, m.tdim);
+  std::string s = "<?xml version=\"1.0\"?>\n<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n"
+                  "<Xdmf Version=\"3.0\" xmlns:xi=\"http://www.w3.org/2001/XInclude\">\n  <Domain>\n"
+                  "    <Grid Name=\"mesh\" GridType=\"Uniform\">\n";
+  const int nvc = m.tdim + 1;
+  s += "      <Topology NumberOfElements=\"" + std::to_string(m.nc) + "\" TopologyType=\"" +
+       (m.tdim == 3 ? "Tetrahedron" : "Triangle") + "\" NodesPerElement=\"" + std::to_string(nvc) + "\">\n";
+  s += "        <DataItem Dimensions=\"" + std::to_string(m.nc) + " " + std::to_string(nvc) +
+       "\" NumberType=\"UInt\" Format=\"XML\">";
+  for (int64_t c = 0; c < m.nc; ++c) {
+    s += "\n";
+    for (int a = 0; a < nvc; ++a) s += (a ? " " : "") + std::to_string(m.cells[c * nvc + a]);
+  }
+  s += "\n        </DataItem>\n      </Topology>\n";
+  s += std::string("      <Geometry GeometryType=\"") + (m.tdim == 3 ? "XYZ" : "XY") + "\">\n";
+  s += "        <DataItem Dimensions=\"" + std::to_string(m.nv) + " " + std::to_string(m.tdim) + "\" Format=\"XML\">";
+  for (int64_t v = 0; v < m.nv; ++v) {
+    s += "\n";
+    for (int r = 0; r < m.tdim; ++r) s += (r ? " " : "") + fmt17(m.x[v * m.tdim + r]);
+  }
+  s += "\n        </DataItem>\n      </Geometry>\n";
+  if (values) {
+    const int ncomp = value_size == 1 ? 1 : 3;  // XDMF vectors are 3-component
+    s += std::string("      <Attribute Name=\"") + (name && *name ? name : "f") + "\" AttributeType=\"" +
+         (value_size == 1 ? "Scalar" : "Vector") + "\" Center=\"Node\">\n";
+    s += "        <DataItem Dimensions=\"" + std::to_string(m.nv) + " " + std::to_string(ncomp) + "\" Format=\"XML\">";
+    for (int64_t v = 0; v < m.nv; ++v) {
+      s += "\n";
+      for (int c = 0; c < ncomp; ++c)
+        s += (c ? " " : "") + fmt17(c < value_size ? values[v * value_size + c] : 0.0);
+    }
+    s += "\n        </DataItem>\n      </Attribute>\n";
+  }
+  s += "    </Grid>\n  </Domain>\n</Xdmf>\n";
   write_file(path, s);
 }
 

@@ -123,6 +123,16 @@ int db2_mesh_destroy(db2_mesh m);
 int db2_mesh_read_xml(const char* path, db2_mesh* out);
 /* File(filename) << mesh. */
 int db2_mesh_write_xml(db2_mesh m, const char* path);
+/* XDMFFile(path).read(mesh) / .write(mesh) with Encoding.ASCII
+   (dolfin/io/XDMFFile.cpp:91-131, 1140-1930): Topology/Geometry DataItems
+   inline (Format="XML"); HDF5-backed files are rejected (no HDF5 in this
+   build).  Cell vertex lists are sorted on reading.  With values != NULL
+   (host, nv x value_size, value_size 1 or tdim) a vertex field named `name`
+   is written as a node-centred Attribute, as XDMFFile::write(Function)
+   does for a P1 function (:311-397). */
+int db2_mesh_read_xdmf(const char* path, db2_mesh* out);
+int db2_mesh_write_xdmf(db2_mesh m, const char* path, const double* values, int value_size,
+                        const char* name);
 /* File(filename) << vector / >> vector for a host array x[n]; read with
    x = NULL returns the size in *n, else reads at most *n values. */
 int db2_vector_write_xml(const char* path, int64_t n, const double* x);

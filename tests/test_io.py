@@ -73,3 +73,98 @@ def test_bad_files_raise(tmp_path):
         d2.Mesh(str(p))
     with pytest.raises(NotImplementedError):
         d2.File(str(tmp_path / "m.pvd"))
+
+
+# A two-triangle mesh in the layout XDMFFile::write(mesh, Encoding::ASCII)
+# produces (dolfin/io/XDMFFile.cpp add_mesh / add_topology_data /
+# add_geometry_data / add_data_item), vertex lists deliberately unsorted.
+TRI_XDMF = """<?xml version="1.0"?>
+<!DOCTYPE Xdmf SYSTEM "Xdmf.dtd" []>
+<Xdmf Version="3.0" xmlns:xi="http://www.w3.org/2001/XInclude">
+  <Domain>
+    <Grid Name="mesh" GridType="Uniform">
+      <Topology NumberOfElements="2" TopologyType="Triangle" NodesPerElement="3">
+        <DataItem Dimensions="2 3" NumberType="UInt" Format="XML">0 1 3
+2 3 0</DataItem>
+      </Topology>
+      <Geometry GeometryType="XY">
+        <DataItem Dimensions="4 2" Format="XML">0 0
+1 0
+1 1
+0 1</DataItem>
+      </Geometry>
+    </Grid>
+  </Domain>
+</Xdmf>
+"""
+
+
+def test_read_xdmf_ascii_mesh(tmp_path):
+    p = tmp_path / "two.xdmf"
+    p.write_text(TRI_XDMF)
+    m = d2.Mesh(str(p))
+    assert m.num_vertices() == 4 and m.num_cells() == 2
+    assert m.cells().tolist() == [[0, 1, 3], [0, 2, 3]]  # sorted, as Mesh::order leaves them
+    assert np.array_equal(m.coordinates(), [[0, 0], [1, 0], [1, 1], [0, 1]])
+    m2 = d2.UnitSquareMesh(1, 1)
+    with d2.XDMFFile(str(p)) as f:
+        f.read(m2)  # XDMFFile.read(mesh) replaces the mesh's contents
+    assert m2.num_cells() == 2 and np.array_equal(m2.cells(), m.cells())
+
+
+@pytest.mark.parametrize("tdim", [2, 3])
+def test_xdmf_mesh_round_trip_is_exact(tmp_path, tdim):
+    from dolfin_b200 import synthetic
+    m = d2.UnitSquareMesh(5, 4) if tdim == 2 else d2.UnitCubeMesh(3, 2, 2)
+    m.set_coordinates(synthetic.jitter_interior(m.coordinates(), 4, 0.2, 3))
+    p = tmp_path / "m.xdmf"
+    with d2.XDMFFile(str(p)) as f:
+        f.write(m)
+    text = p.read_text()
+    assert ('TopologyType="Tetrahedron"' if tdim == 3 else 'TopologyType="Triangle"') in text
+    assert 'Format="XML"' in text and 'NumberType="UInt"' in text
+    m2 = d2.Mesh(str(p))
+    assert np.array_equal(m2.cells(), m.cells())
+    assert np.array_equal(m2.coordinates(), m.coordinates())  # 17 significant digits
+
+
+def test_xdmf_p1_function_attribute(tmp_path):
+    import xml.etree.ElementTree as ET
+    m = d2.UnitCubeMesh(2, 2, 2)
+    W = d2.FunctionSpace(m, "Lagrange", 1)
+    vals = np.arange(m.num_vertices(), dtype=np.float64) * 0.5
+    f = d2.Function(W, vals, name="kappa")
+    p = tmp_path / "f.xdmf"
+    d2.XDMFFile(str(p)).write(f)
+    root = ET.parse(p).getroot()
+    attr = root.find("./Domain/Grid/Attribute")
+    assert attr.get("Name") == "kappa" and attr.get("Center") == "Node"
+    assert attr.get("AttributeType") == "Scalar"
+    got = np.array(attr.find("DataItem").text.split(), dtype=np.float64)
+    assert np.array_equal(got, vals)
+    V = d2.VectorFunctionSpace(m, "Lagrange", 1)
+    u = d2.Function(V, np.arange(V.dim(), dtype=np.float64), name="u")
+    d2.XDMFFile(str(p)).write(u)
+    attr = ET.parse(p).getroot().find("./Domain/Grid/Attribute")
+    assert attr.get("AttributeType") == "Vector"
+    got = np.array(attr.find("DataItem").text.split(), dtype=np.float64).reshape(-1, 3)
+    nv = m.num_vertices()
+    assert np.array_equal(got, np.arange(3 * nv, dtype=np.float64).reshape(3, nv).T)
+
+
+def test_xdmf_rejects_hdf5_and_bad_files(tmp_path):
+    p = tmp_path / "h5.xdmf"
+    p.write_text(TRI_XDMF.replace('NumberType="UInt" Format="XML"', 'NumberType="UInt" Format="HDF"'))
+    with pytest.raises(_capi.DB2Error, match="HDF5"):
+        d2.Mesh(str(p))
+    p.write_text(TRI_XDMF.replace('Dimensions="2 3"', 'Dimensions="3 3"'))
+    with pytest.raises(_capi.DB2Error, match="DataItem holds"):
+        d2.Mesh(str(p))
+    p.write_text(TRI_XDMF.replace("2 3 0</DataItem>", "2 3 7</DataItem>"))
+    with pytest.raises(_capi.DB2Error, match="vertex"):
+        d2.Mesh(str(p))
+    p.write_text(TRI_XDMF.replace('TopologyType="Triangle"', 'TopologyType="Quadrilateral"'))
+    with pytest.raises(_capi.DB2Error, match="TopologyType"):
+        d2.Mesh(str(p))
+    with pytest.raises(NotImplementedError):
+        d2.XDMFFile(str(tmp_path / "x.xdmf")).write(d2.UnitSquareMesh(1, 1), encoding=d2.XDMFFile.Encoding.HDF5)
