@@ -57,6 +57,7 @@ _SIGS = {
     "db2_mesh_read_xml": [C.c_char_p, PP],
     "db2_mesh_write_xml": [P, C.c_char_p],
     "db2_mesh_read_xdmf": [C.c_char_p, PP],
+    "db2_pattern_set_row_range": [P, C.c_int64, C.c_int64],
     "db2_mesh_write_xdmf": [P, C.c_char_p, P, C.c_int, C.c_char_p],
     "db2_vector_write_xml": [C.c_char_p, I64, P],
     "db2_vector_read_xml": [C.c_char_p, C.POINTER(I64), P],

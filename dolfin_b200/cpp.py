@@ -311,6 +311,11 @@ class SparsityPattern(_Handle):
         """Launch shape of the assembly kernel (see db2_pattern_retile)."""
         call("db2_pattern_retile", self._h, int(tile_threads), int(seg_cap_bytes))
 
+    def set_row_range(self, node_begin, node_end):
+        """Assemble only the rows of nodes [node_begin, node_end) (a rank's
+        share of a row-partitioned assembly; see db2_pattern_set_row_range)."""
+        call("db2_pattern_set_row_range", self._h, int(node_begin), int(node_end))
+
 
 def _wrap_device(ptr, n, dtype, owner):
     """Zero-copy torch view of device memory owned by `owner` (kept alive)."""

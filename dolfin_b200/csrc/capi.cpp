@@ -343,6 +343,13 @@ int db2_pattern_retile(db2_pattern P, int tile_threads, int seg_cap_bytes) {
   });
 }
 
+int db2_pattern_set_row_range(db2_pattern P, int64_t node_begin, int64_t node_end) {
+  return guard([&] {
+    need(P, "pattern");
+    db2::set_row_range(*P->P, node_begin, node_end);
+  });
+}
+
 int db2_pattern_facet_plan_info(db2_pattern P, int64_t* nbnodes, int64_t* nincidences, int* kf) {
   return guard([&] {
     need(P, "pattern");
@@ -447,6 +454,8 @@ int db2_assemble_facets_bc(db2_pattern P, const db2_form* a_ds, const double* wa
     need(bc_vals, "bc_vals");
     need(b, "b");
     db2::Pattern& Pt = *P->P;
+    if (Pt.row_begin != 0 || Pt.row_end >= 0)
+      db2::fail(DB2_ERR_UNSUPPORTED, "facet terms with a partial row range (db2_pattern_set_row_range)");
     if (a_ds) need(vals, "vals");
     if (Pt.V->reordered()) {
       // natural scratch from zero, the facet terms added there, then gathered

@@ -475,15 +475,16 @@ void canonical_node_map(int tdim, int degree, int li, int* map) {
 // block) per thread whose row segment (one test component) fits
 // seg_cap_doubles.
 
-std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doubles, int* max_seg_out) {
+std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doubles, int* max_seg_out,
+                            int64_t node_begin, int64_t node_end) {
   const int bs = P.bs;
-  const int64_t nn = P.V->nnodes;
+  const int64_t nn = node_end < 0 ? P.V->nnodes : node_end;
   // P2: vertex nodes [0, nv) precede edge nodes; no tile spans both, so the
   // kernel knows each tile's row kind up front
   const int64_t split = P.V->degree == 2 ? P.V->mesh->nv : -1;
   int max_seg = 0;
   std::vector<Tile> comp0;
-  int64_t n0 = 0;
+  int64_t n0 = node_begin;
   while (n0 < nn) {
     int64_t n1 = n0;
     while (n1 < nn) {
@@ -511,8 +512,9 @@ std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doub
 static void build_tiles(Pattern& P, int tile_threads, int seg_cap_doubles) {
   const int bs = P.bs;
   P.tile_threads = tile_threads;
+  P.seg_cap_bytes = seg_cap_doubles * 8;
   int max_seg = 0;
-  std::vector<Tile> all = cut_tiles(P, tile_threads, seg_cap_doubles, &max_seg);
+  std::vector<Tile> all = cut_tiles(P, tile_threads, seg_cap_doubles, &max_seg, P.row_begin, P.row_end);
   P.seg_cap = max_seg;
   // Group tiles by the shared memory their row segment needs, so that small
   // (e.g. edge-node) tiles are not launched with the largest tile's
@@ -546,6 +548,23 @@ void retile(Pattern& P, int tile_threads, int seg_cap_bytes) {
   if (seg_cap_bytes < 1024 || seg_cap_bytes > 220 * 1024)
     fail(DB2_ERR_ARGUMENT, "seg_cap_bytes out of range");
   build_tiles(P, tile_threads, seg_cap_bytes / 8);
+  if (P.on_device) P.d_tiles.upload(P.tiles.data(), P.tiles.size() * sizeof(Tile));
+}
+
+// Row-partitioned assembly: a rank assembles the node rows [node_begin,
+// node_end) completely from the cells around them (their incidence lists),
+// with no exchange -- the row-owner analogue of DOLFIN's owned-row ranges
+// (SparsityPattern.cpp:200-255).  Only the tile kernel is restricted.
+void set_row_range(Pattern& P, int64_t node_begin, int64_t node_end) {
+  const int64_t nn = P.V->nnodes;
+  if (node_begin < 0 || node_end < node_begin || node_end > nn)
+    fail(DB2_ERR_ARGUMENT, "row range [%lld, %lld) outside [0, %lld)", (long long)node_begin,
+         (long long)node_end, (long long)nn);
+  if (P.V->reordered() && !(node_begin == 0 && node_end == nn))
+    fail(DB2_ERR_UNSUPPORTED, "row ranges are provided for the natural numbering");
+  P.row_begin = node_begin;
+  P.row_end = node_end == nn ? -1 : node_end;
+  build_tiles(P, P.tile_threads, P.seg_cap_bytes / 8);
   if (P.on_device) P.d_tiles.upload(P.tiles.data(), P.tiles.size() * sizeof(Tile));
 }
 

@@ -134,6 +134,10 @@ struct Pattern {
   std::vector<int32_t> class_begin;  // tiles[class_begin[k] .. class_begin[k+1]) share
   std::vector<int32_t> class_smem;   //   a launch with class_smem[k] bytes of smem
   int tile_threads = 128;            // CTA size of the tile kernel
+  int seg_cap_bytes = 0;             // row-segment cap the tiles were cut with
+  // node rows the tile kernel assembles: [row_begin, row_end) (a rank's share
+  // of a row-partitioned assembly); row_end < 0 = all rows
+  int64_t row_begin = 0, row_end = -1;
 
   int seg_cap = 0;                   // doubles of shared memory of the largest tile
   // Device incidence records (rs = 8 or 16 bytes, one vector load each):
@@ -193,7 +197,9 @@ void build_facet_plan(Pattern& P);
 // Re-cut the tiles of an existing plan (autotuning), re-uploading d_tiles.
 void retile(Pattern& P, int tile_threads, int seg_cap_bytes);
 // Tiles of a pattern for a launch shape (pure; does not modify P).
-std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doubles, int* max_seg);
+std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doubles, int* max_seg,
+                            int64_t node_begin = 0, int64_t node_end = -1);
+void set_row_range(Pattern& P, int64_t node_begin, int64_t node_end);
 
 // Launchers (kernels.cu).  All return after enqueueing on `stream`.
 struct FormArgs {

@@ -193,6 +193,17 @@ int db2_pattern_facet_plan_copy(db2_pattern P, uint32_t* bnode, uint32_t* binc_p
    tile_threads threads, row segments of at most seg_cap_bytes of shared
    memory.  Results do not depend on the launch shape (bitwise). */
 int db2_pattern_retile(db2_pattern P, int tile_threads, int seg_cap_bytes);
+/* Row-partitioned assembly (one rank's share of a single mesh): from now on
+   the matrix / system entry points (db2_assemble_matrix, _system, _system_bc)
+   compute and write only the CSR rows and b entries of nodes
+   [node_begin, node_end), every component, each from all cells around it,
+   so no exchange between ranks is needed -- the counterpart of the owned
+   row range of DOLFIN's distributed SparsityPattern
+   (dolfin/la/SparsityPattern.cpp:200-255, SparsityPattern::apply :441),
+   whose off-process entries this design never produces.  Other rows are left
+   as they were.  [0, nnodes) restores full assembly.  Natural numbering
+   only; facet terms (db2_assemble_facets*) need the full range. */
+int db2_pattern_set_row_range(db2_pattern P, int64_t node_begin, int64_t node_end);
 
 /* ---- assembly --------------------------------------------------------- */
 /* Assembler::assemble(A, a) (dolfin/fem/Assembler.cpp:52-103) for a bilinear

@@ -254,3 +254,24 @@ def test_new_entry_points_reject_bad_arguments():
     with pytest.raises(NotImplementedError):
         d2.assemble_action(d2.TrialFunction(V) * d2.TestFunction(V) * d2.ds, d2.Vector.__new__(d2.Vector))
 
+
+
+def test_row_range_tiles_cover_exactly_the_range():
+    """A rank's row range (row-partitioned assembly): the tiles cover exactly
+    the nodes [begin, end), for every component, with no overlap."""
+    m = d2.UnitCubeMesh(3, 3, 3)
+    V = d2.VectorFunctionSpace(m, "Lagrange", 2)
+    P = V.pattern()
+    nn = V.dim() // 3
+    for a, b in [(0, nn), (5, 77), (0, 0), (nn - 3, nn), (m.num_vertices() - 2, m.num_vertices() + 9)]:
+        P.set_row_range(a, b)
+        t = P.plan()["tiles"]
+        for c in range(3):
+            tc = t[t[:, 0] == c]
+            covered = np.concatenate([np.arange(n0, n1) for _, n0, n1, _ in tc]) if len(tc) else np.array([], int)
+            assert np.array_equal(np.sort(covered), np.arange(a, b))
+    P.set_row_range(0, nn)
+    assert len(P.plan()["tiles"]) > 0
+    for a, b in [(-1, 3), (5, 4), (0, nn + 1)]:
+        with pytest.raises(_capi.DB2Error):
+            P.set_row_range(a, b)
