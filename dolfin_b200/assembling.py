@@ -16,7 +16,7 @@ import ctypes as C
 from . import _capi
 from ._capi import call
 from .la import Matrix, Vector
-from .ufl import Form, Recognised, recognise, recognise_functional, recognise_parts
+from .ufl import Form, Recognised, recognise_functional, recognise_parts
 
 _PREC = {"fp64": _capi.FP64, "fp32": _capi.FP32_CONTRACT, None: _capi.FP64}
 
@@ -39,6 +39,18 @@ def _coeff_ptr(rec):
     return _ptr(f.vertex_tensor())
 
 
+def _parts(form):
+    """recognise_parts(form), computed once per Form object (forms and
+    Constants are immutable; Functions are read through their device
+    tensors at each call), so repeated assemblies spend no host time on
+    recognition."""
+    parts = getattr(form, "_db2_parts", None)
+    if parts is None:
+        parts = recognise_parts(form)
+        form._db2_parts = parts
+    return parts
+
+
 def _check_tensor_dims(tensor, rec):
     # AssemblerBase::init_global_tensor, dolfin/fem/AssemblerBase.cpp:182-191
     if tensor.size(0) != rec.V.dim():
@@ -57,7 +69,7 @@ def assemble(form, tensor=None, form_compiler_parameters=None, add_values=False,
         raise TypeError("expected a Form")
     if form.rank() == 0:
         return _assemble_scalar(form)
-    cell, facet = recognise_parts(form)
+    cell, facet = _parts(form)
     rec = cell or facet
     prec = _PREC[precision]
     parts = [r for r in (cell, facet) if r is not None]
@@ -95,7 +107,7 @@ def assemble_local(form, cell):
         raise TypeError("expected a Form")
     if form.rank() == 0:
         raise NotImplementedError("assemble_local of a functional is not provided")
-    cell_rec, facet_rec = recognise_parts(form)
+    cell_rec, facet_rec = _parts(form)
     rec = cell_rec or facet_rec
     V = rec.V
     idx = np.atleast_1d(np.asarray(cell, dtype=np.int64))
@@ -139,8 +151,8 @@ class SystemAssembler:
     (dolfin/fem/SystemAssembler.cpp:138-301, cell_wise_assembly :303-492)."""
 
     def __init__(self, a, L, bcs=None, precision="fp64"):
-        self.ra, self.ra_ds = recognise_parts(a)
-        self.rL, self.rL_ds = recognise_parts(L)
+        self.ra, self.ra_ds = _parts(a)
+        self.rL, self.rL_ds = _parts(L)
         if self.ra is None:
             raise NotImplementedError("the bilinear form needs a cell (dx) part")
         if self.rL is None:
@@ -217,7 +229,7 @@ def assemble_action(a, x, y=None, precision="fp64"):
     """Matrix-free y = A(a) x without forming A (replaces assemble + GenericMatrix::mult)."""
     if "ds" in a.measures():
         raise NotImplementedError("matrix-free action of ds terms is not provided")
-    rec = recognise(a)
+    rec = _parts(a)[0]
     xt = x.tensor() if hasattr(x, "tensor") else x
     if xt.numel() != rec.V.dim():
         raise RuntimeError("x has the wrong size")

@@ -409,6 +409,24 @@ void launch_apply(const Pattern& P, const FormArgs& a, int precision, const doub
   fail(DB2_ERR_UNSUPPORTED, "matrix-free action not provided for this form/element");
 }
 
+void preload_vjp_kernels() {
+  cudaFuncAttributes at;
+  cudaError_t e = cudaSuccess;
+  auto get = [&](const void* f) {
+    const cudaError_t r = cudaFuncGetAttributes(&at, f);
+    if (r != cudaSuccess) e = r;
+  };
+#define DB2_VJP_LOAD(D_, P_)                                                  \
+  get((const void*)dev::k_vjp_cells<D_, P_, true, float>);                    \
+  get((const void*)dev::k_vjp_cells<D_, P_, true, double>);                   \
+  get((const void*)dev::k_vjp_cells<D_, P_, false, float>);                   \
+  get((const void*)dev::k_vjp_cells<D_, P_, false, double>);                  \
+  get((const void*)dev::k_vjp_vertices<D_, P_>);
+  DB2_VJP_LOAD(3, 1) DB2_VJP_LOAD(3, 2) DB2_VJP_LOAD(2, 1) DB2_VJP_LOAD(2, 2)
+#undef DB2_VJP_LOAD
+  if (e != cudaSuccess) fail(DB2_ERR_CUDA, "loading the adjoint kernels: %s", cudaGetErrorString(e));
+}
+
 size_t vjp_scratch_doubles(const Pattern& P) {
   return size_t(P.V->mesh->nc) * (P.V->mesh->tdim + 1);
 }

@@ -454,8 +454,6 @@ int db2_assemble_facets_bc(db2_pattern P, const db2_form* a_ds, const double* wa
     need(bc_vals, "bc_vals");
     need(b, "b");
     db2::Pattern& Pt = *P->P;
-    if (Pt.row_begin != 0 || Pt.row_end >= 0)
-      db2::fail(DB2_ERR_UNSUPPORTED, "facet terms with a partial row range (db2_pattern_set_row_range)");
     if (a_ds) need(vals, "vals");
     if (Pt.V->reordered()) {
       // natural scratch from zero, the facet terms added there, then gathered

@@ -19,6 +19,8 @@
 // same summation order on every run.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "facet_rows.cuh"
 
 namespace db2 {
@@ -39,7 +41,10 @@ struct FacetParams {
   double* b;
   const uint8_t* bc_flags;   // dof-level Dirichlet flags or null
   const double* bc_vals;
-  int64_t nnodes, nverts, nbnodes;
+  int64_t nnodes, nverts;
+  // boundary nodes handled by this launch: bnode[bn0 .. bn0 + nbnodes), the
+  // ones inside the pattern's row range
+  int64_t bn0, nbnodes;
   int bs;
 };
 
@@ -59,8 +64,9 @@ __device__ __forceinline__ void load_facet(const FacetParams& p, uint32_t s, boo
 // |F| * row, Dirichlet rows excepted (their b entry is the boundary value).
 template <int D, int P, bool WP1>
 __global__ void __launch_bounds__(256) k_facet_vector(const FacetParams p) {
-  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= p.nbnodes) return;
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= p.nbnodes) return;
+  const int64_t t = p.bn0 + i;
   const uint32_t node = __ldg(p.bnode + t);
   const bool vertex = P == 1 || node < p.nverts;
   double acc = 0.0;
@@ -85,8 +91,9 @@ __global__ void __launch_bounds__(256) k_facet_vector(const FacetParams p) {
 template <int D, int P, bool WP1>
 __global__ void __launch_bounds__(256) k_facet_matrix(const FacetParams p) {
   constexpr int KF = FacetRows<D, P>::KF;
-  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= p.nbnodes) return;
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= p.nbnodes) return;
+  const int64_t t = p.bn0 + i;
   const uint32_t node = __ldg(p.bnode + t);
   if (p.bc_flags && __ldg(p.bc_flags + node)) return;
   const bool vertex = P == 1 || node < p.nverts;
@@ -248,9 +255,30 @@ dev::FacetParams facet_params(Pattern& P) {
   p.cols = P.d_cols.as<int32_t>();
   p.nnodes = P.V->nnodes;
   p.nverts = m.nv;
-  p.nbnodes = int64_t(F.bnode.size());
+  // a partial row range (db2_pattern_set_row_range) takes the boundary nodes
+  // inside it only: their facet rows are complete there, like the cell rows
+  const int64_t r0 = P.row_begin, r1 = P.row_end < 0 ? P.V->nnodes : P.row_end;
+  const auto lo = std::lower_bound(F.bnode.begin(), F.bnode.end(), uint32_t(r0));
+  const auto hi = std::lower_bound(F.bnode.begin(), F.bnode.end(), uint32_t(r1));
+  p.bn0 = int64_t(lo - F.bnode.begin());
+  p.nbnodes = int64_t(hi - lo);
   p.bs = P.V->vsize;
   return p;
+}
+
+// Zero the pattern's rows inside its row range (all of them by default):
+// CSR values of a scalar pattern, or the b entries (c, node) of every
+// component c.
+void zero_range_values(const Pattern& P, double* vals, cudaStream_t s) {
+  const int64_t r0 = P.row_begin, r1 = P.row_end < 0 ? P.V->nnodes : P.row_end;
+  const int64_t v0 = P.node_rowptr[r0], v1 = P.node_rowptr[r1];
+  if (v1 > v0) cudaMemsetAsync(vals + v0, 0, size_t(v1 - v0) * sizeof(double), s);
+}
+void zero_range_dofs(const Pattern& P, double* b, cudaStream_t s) {
+  const int64_t r0 = P.row_begin, r1 = P.row_end < 0 ? P.V->nnodes : P.row_end;
+  if (r1 <= r0) return;
+  for (int c = 0; c < P.V->vsize; ++c)
+    cudaMemsetAsync(b + int64_t(c) * P.V->nnodes + r0, 0, size_t(r1 - r0) * sizeof(double), s);
 }
 
 template <typename K>
@@ -278,7 +306,7 @@ void launch_facet_vector(Pattern& P, const FormArgs& L, double* b, bool add_valu
   p.w = L.w;
   p.b = b;
   p.bc_flags = bc_flags;
-  if (!add_values) cudaMemsetAsync(b, 0, size_t(P.V->dim()) * sizeof(double), s);
+  if (!add_values) zero_range_dofs(P, b, s);
 #define DB2_FV(D_, P_)                                                                   \
   if (D == D_ && deg == P_) {                                                            \
     if (wp1) launch_rows(dev::k_facet_vector<D_, P_, true>, p, s);                       \
@@ -305,7 +333,7 @@ void launch_facet_matrix(Pattern& P, const FormArgs& a, double* vals, bool add_v
   p.b = b;
   p.bc_flags = bc_flags;
   p.bc_vals = bc_vals;
-  if (!add_values) cudaMemsetAsync(vals, 0, size_t(P.nnz) * sizeof(double), s);
+  if (!add_values) zero_range_values(P, vals, s);
 #define DB2_FM(D_, P_)                                                                   \
   if (D == D_ && deg == P_) {                                                            \
     if (wp1) launch_rows(dev::k_facet_matrix<D_, P_, true>, p, s);                       \

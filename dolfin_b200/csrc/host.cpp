@@ -742,6 +742,7 @@ void Pattern::ensure_device() {
   d_cell_inc.upload(cell_inc.data(), cell_inc.size() * sizeof(uint32_t));
   d_tiles.upload(tiles.data(), tiles.size() * sizeof(Tile));
   launch_expand_csr(*this);
+  noalloc_prepare_device();
   on_device = true;
 }
 

@@ -227,5 +227,11 @@ void launch_expand_csr(const Pattern& P);
 void count_launch(int n = 1);
 void check_cuda(const char* what);
 size_t vjp_scratch_doubles(const Pattern& P);
+// Load the adjoint kernels onto the current device (lazy module loading
+// would otherwise do it, allocating, at their first launch).
+void preload_vjp_kernels();
+// Once per device: set up the allocation-free adjoint's fixed scratch array
+// (vjp_noalloc.cu); called by Pattern::ensure_device.
+void noalloc_prepare_device();
 
 }  // namespace db2

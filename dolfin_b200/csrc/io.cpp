@@ -13,6 +13,7 @@
 // their vertices sorted ascending, as MeshEditor::close -> Mesh::order leaves
 // a freshly read mesh (TetrahedronCell::order, dolfin/mesh/TetrahedronCell.cpp:455).
 #include <algorithm>
+#include <limits>
 #include <cctype>
 #include <cstdio>
 #include <cstdlib>
@@ -234,13 +235,19 @@ std::vector<int64_t> dims_of(const Tag& t, const char* path) {
   std::istringstream in(need_attr(t, "Dimensions"));
   int64_t v;
   while (in >> v) d.push_back(v);
-  if (d.size() != 2 || d[0] < 0 || d[1] <= 0) fail(DB2_ERR_ARGUMENT, "%s: bad DataItem Dimensions", path);
+  if (d.size() != 2 || d[0] < 0 || d[1] <= 0 || d[1] > 16 || d[0] > (int64_t(1) << 40))
+    fail(DB2_ERR_ARGUMENT, "%s: bad DataItem Dimensions", path);
   return d;
 }
 
 template <typename T>
 std::vector<T> numbers(const std::string& s, const Tag& t, size_t count, const char* path) {
   const size_t end = s.find('<', t.body);
+  // every value takes at least one character of the file, so Dimensions
+  // beyond that are refused before reserving
+  const size_t avail = (end == std::string::npos ? s.size() : end) - t.body;
+  if (count > avail + 1)
+    fail(DB2_ERR_SHAPE, "%s: DataItem Dimensions (%zu values) exceed its data", path, count);
   std::vector<T> v;
   v.reserve(count);
   const char* p = s.c_str() + t.body;
@@ -255,7 +262,8 @@ std::vector<T> numbers(const std::string& s, const Tag& t, size_t count, const c
       v.push_back(T(x));
     } else {
       const long long x = std::strtoll(p, &e, 10);
-      if (e == p || x < 0) fail(DB2_ERR_ARGUMENT, "%s: bad index in DataItem", path);
+      if (e == p || x < 0 || (unsigned long long)x > (unsigned long long)std::numeric_limits<T>::max())
+        fail(DB2_ERR_ARGUMENT, "%s: bad index in DataItem", path);
       v.push_back(T(x));
     }
     p = e;

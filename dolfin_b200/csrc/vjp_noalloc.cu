@@ -22,8 +22,7 @@ std::shared_ptr<Pattern> pattern_of(db2_pattern P);
 int guard_call(const std::function<void()>& f);
 
 // Largest work array the entry point can use: C (d+1) doubles, i.e. up to
-// 524,288 tetrahedra or 699,050 triangles.  Every GPU that loads the library
-// holds these 16 MiB until the process exits.
+// 524,288 tetrahedra or 699,050 triangles.
 constexpr size_t kNoAllocScratchDoubles = size_t(1) << 21;
 static __device__ __align__(256) double g_vjp_scratch[kNoAllocScratchDoubles];
 
@@ -31,23 +30,45 @@ namespace {
 std::mutex g_mutex;
 constexpr int kMaxDevices = 64;
 double* g_scratch_addr[kMaxDevices] = {};
+}  // namespace
 
-// The device address of g_vjp_scratch on the current device.  In host code
-// the array's name is only a host-side stand-in, so the address is looked up
-// once per device (with that device current) and cached.
+// Set-up, once per device, with that device current; called when a pattern
+// is first made resident (Pattern::ensure_device), which allocates anyway.
+// With lazy module loading (the CUDA 12 default) the 16 MiB array and the
+// adjoint kernels reach the device only when first used; looking the array
+// up here and loading the kernels here keeps that out of the entry point.
+// In host code the array's name is only a host-side stand-in, so its device
+// address is looked up (cudaGetSymbolAddress) and cached per device.  From
+// then on the device holds the array until the process exits.
+void noalloc_prepare_device() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) fail(DB2_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return;  // such devices refuse the entry point instead
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (g_scratch_addr[dev]) return;
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_vjp_scratch);
+  if (e != cudaSuccess || !p)
+    fail(DB2_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+  preload_vjp_kernels();
+  g_scratch_addr[dev] = static_cast<double*>(p);
+}
+
+namespace {
+// The cached device address of g_vjp_scratch on the current device; never
+// looks it up (that could load the module, i.e. allocate).
 double* scratch_on_current_device() {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) fail(DB2_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) fail(DB2_ERR_UNSUPPORTED, "device index %d", dev);
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_vjp_scratch);
-    if (e != cudaSuccess || !p)
-      fail(DB2_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
-    g_scratch_addr[dev] = static_cast<double*>(p);
-  }
+  if (!g_scratch_addr[dev])
+    fail(DB2_ERR_ARGUMENT,
+         "db2_vjp_kappa_noalloc: no pattern has been made resident on device %d yet (its "
+         "fixed scratch array is set up then); assemble with the pattern on this device first",
+         dev);
   return g_scratch_addr[dev];
 }
 }  // namespace

@@ -194,15 +194,17 @@ int db2_pattern_facet_plan_copy(db2_pattern P, uint32_t* bnode, uint32_t* binc_p
    memory.  Results do not depend on the launch shape (bitwise). */
 int db2_pattern_retile(db2_pattern P, int tile_threads, int seg_cap_bytes);
 /* Row-partitioned assembly (one rank's share of a single mesh): from now on
-   the matrix / system entry points (db2_assemble_matrix, _system, _system_bc)
-   compute and write only the CSR rows and b entries of nodes
+   the assembly entry points (db2_assemble_matrix, _vector, _system,
+   _system_bc, _facets_bc; cell and exterior-facet terms alike) compute and
+   write -- or zero, where add_values = 0 -- only the CSR rows and b entries
+   of nodes
    [node_begin, node_end), every component, each from all cells around it,
    so no exchange between ranks is needed -- the counterpart of the owned
    row range of DOLFIN's distributed SparsityPattern
    (dolfin/la/SparsityPattern.cpp:200-255, SparsityPattern::apply :441),
    whose off-process entries this design never produces.  Other rows are left
    as they were.  [0, nnodes) restores full assembly.  Natural numbering
-   only; facet terms (db2_assemble_facets*) need the full range. */
+   only. */
 int db2_pattern_set_row_range(db2_pattern P, int64_t node_begin, int64_t node_end);
 
 /* ---- assembly --------------------------------------------------------- */
@@ -285,12 +287,14 @@ int db2_vjp_kappa(db2_pattern P, const db2_form* a, const double* kappa, const d
    db2_vjp_kappa, but the work array is a fixed array inside the library:
    at most 2^21 doubles, i.e. cells * (tdim + 1) <= 2097152 (524,288
    tetrahedra / 699,050 triangles); larger patterns fail with DB2_ERR_SHAPE.
-   It calls no cudaMalloc/cudaFree: the pattern must already be resident on
-   the device (after any assembly with it, or db2_pattern_csr_device).  The
-   first call on each device looks up the array's device address
-   (cudaGetSymbolAddress) and should come before any stream capture.  All
-   calls share the one array, so calls that overlap on the GPU (other
-   streams, other threads) race; order them on one stream. */
+   It calls no cudaMalloc/cudaFree and loads nothing: the pattern must
+   already be resident on the current device (after any assembly with it, or
+   db2_pattern_csr_device).  Making a pattern resident sets the array up on
+   that device (cudaGetSymbolAddress, which with lazy module loading is when
+   the 16 MiB reach the device) and loads the adjoint kernels; the device
+   holds the array from then until the process exits.  All calls share the
+   one array, so calls that overlap on the GPU (other streams, other
+   threads) race; order them on one stream. */
 int db2_vjp_kappa_noalloc(db2_pattern P, const db2_form* a, const double* kappa,
                           const db2_form* L, const double* f, const double* gA,
                           const double* gb, int precision, double* dkappa, void* stream);

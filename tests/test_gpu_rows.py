@@ -33,12 +33,17 @@ def _problem(kind):
         u, v = d2.TrialFunction(V), d2.TestFunction(V)
         a = kappa * d2.inner(d2.grad(u), d2.grad(v)) * d2.dx
         L = f * v * d2.dx
+        if "ds" in kind:
+            # exterior-facet terms: boundary mass and a P1 Neumann load
+            a = a + d2.Constant(0.5) * u * v * d2.ds
+            L = L + kappa * v * d2.ds
         if kind.endswith("bc"):
-            bcs = d2.DirichletBC(V, 0.25, "on_boundary")
+            where = "on_boundary" if "ds" not in kind else (lambda x, on: on and x[0] < 1e-12)
+            bcs = d2.DirichletBC(V, 0.25, where)
     return V, a, L, bcs
 
 
-@pytest.mark.parametrize("kind", ["p2", "elas", "p1bc", "p2bc"])
+@pytest.mark.parametrize("kind", ["p2", "elas", "p1bc", "p2bc", "p1ds", "p2ds", "p1dsbc"])
 @pytest.mark.parametrize("nranks", [2, 3])
 def test_row_partitioned_assembly_equals_full(kind, nranks):
     V, a, L, bcs = _problem(kind)

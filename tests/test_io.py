@@ -163,6 +163,14 @@ def test_xdmf_rejects_hdf5_and_bad_files(tmp_path):
     p.write_text(TRI_XDMF.replace("2 3 0</DataItem>", "2 3 7</DataItem>"))
     with pytest.raises(_capi.DB2Error, match="vertex"):
         d2.Mesh(str(p))
+    # an index beyond 32 bits is refused, not wrapped to a valid vertex
+    p.write_text(TRI_XDMF.replace("2 3 0</DataItem>", "2 3 4294967296</DataItem>"))
+    with pytest.raises(_capi.DB2Error, match="bad index"):
+        d2.Mesh(str(p))
+    # Dimensions larger than the data can hold are refused before reserving
+    p.write_text(TRI_XDMF.replace('Dimensions="2 3"', 'Dimensions="1000000000000 3"'))
+    with pytest.raises(_capi.DB2Error, match="exceed its data"):
+        d2.Mesh(str(p))
     p.write_text(TRI_XDMF.replace('TopologyType="Triangle"', 'TopologyType="Quadrilateral"'))
     with pytest.raises(_capi.DB2Error, match="TopologyType"):
         d2.Mesh(str(p))

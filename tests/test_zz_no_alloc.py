@@ -5,8 +5,9 @@ during a call -- applications that own all device memory through their own
 pool allocator, or loops whose concurrently running streams cudaMalloc's
 implicit synchronisation would stall.  This file is named to be collected
 last: it checks the entry point, called through the C ABI, against the
-allocating entry point (db2_vjp_kappa) on two calls in a row, both when run
-alone in a fresh process and after the rest of the suite."""
+allocating entry point (db2_vjp_kappa) on two calls in a row, and that those
+two calls leave the device's free memory unchanged, both when run alone in a
+fresh process and after the rest of the suite."""
 import ctypes as C
 
 import numpy as np
@@ -39,15 +40,24 @@ def test_noalloc_vjp_matches_allocating_entry_point_twice(deg):
     nv = mesh.num_vertices()
     kappa = torch.as_tensor(synthetic.lognormal_field(nv, 0.5, 7), device="cuda")
     f = torch.as_tensor(rng.uniform(-1, 1, nv), device="cuda")
+    # an ordinary assembly makes the pattern resident on the device (which
+    # also sets up the entry point's fixed array there)
+    u, v = d2.TrialFunction(V), d2.TestFunction(V)
+    d2.assemble(d2.inner(d2.grad(u), d2.grad(v)) * d2.dx)
     gA = torch.as_tensor(rng.standard_normal(P.nnz()), device="cuda")
     gb = torch.as_tensor(rng.standard_normal(V.dim()), device="cuda")
+    outs = [torch.full((nv,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(2)]
     ref = torch.empty(nv, dtype=torch.float64, device="cuda")
-    _vjp("db2_vjp_kappa", P, kappa, f, gA, gb, ref)  # also makes the pattern device-resident
     torch.cuda.synchronize()
-    for _ in range(2):
-        out = torch.full((nv,), float("nan"), dtype=torch.float64, device="cuda")
+    free0 = torch.cuda.mem_get_info()[0]
+    for out in outs:
         _vjp("db2_vjp_kappa_noalloc", P, kappa, f, gA, gb, out)
         torch.cuda.synchronize()
+    # nothing was allocated on the device by the two calls
+    assert torch.cuda.mem_get_info()[0] == free0
+    _vjp("db2_vjp_kappa", P, kappa, f, gA, gb, ref)
+    torch.cuda.synchronize()
+    for out in outs:
         err = float((out - ref).abs().max() / ref.abs().max())
         assert err <= 1e-12
 
