@@ -45,6 +45,12 @@ WORKLOADS = {
 }
 
 
+# What the numbers' correctness rests on (the full-size entry-wise parity
+# tests compare these configurations with the oracle).
+PARITY_NOTE = ("oracle-pinned: entry-wise vs the CPU restatement of DOLFIN's assembly at full size "
+               "(P1 values also pinned by the reference's known answers; P2 and vector-P2 values by "
+               "the oracle's independent quadrature only)")
+
 # the adjoint workloads: kappa = exp(g), g ~ N(0, 0.5^2) per vertex
 LOGNORMAL_KAPPA = {"poisson_p1_64", "poisson_p1_96"}
 
@@ -195,11 +201,12 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def setup_workload(name, seed, device):
+def setup_workload(name, seed, device, n_override=None):
     import torch
     import dolfin_b200 as d2
     from dolfin_b200 import synthetic
     kind, n, deg, _ = WORKLOADS[name]
+    n = n_override or n
     t0 = time.perf_counter()
     mesh = d2.UnitCubeMesh(n, n, n)
     x0 = mesh.coordinates()
@@ -256,18 +263,25 @@ def algorithmic_bytes(w):
 
 
 def profiled_traffic(workload):
-    """DRAM bytes (read + write) per step of the assembly kernels, from the
-    committed ncu launch list of this workload (profiles/); None if there is
-    none.  It is a separate one-pass ncu capture, not measured by this run."""
-    path = os.path.join(ROOT, "profiles", f"k_assemble_launches_{workload}.txt")
+    """(DRAM bytes read + written per A+b step of the assembly kernels,
+    source): from the committed ncu launch list of this workload under
+    profiles/ -- a separate one-pass capture, not measured by this run, so
+    the source names the file and the kernel revision it was captured on."""
+    name = f"k_assemble_launches_{workload}.txt"
+    path = os.path.join(ROOT, "profiles", name)
+    traffic, rev = None, None
     try:
         with open(path) as fh:
             for line in fh:
                 if line.startswith("traffic_bytes_per_step:"):
-                    return int(line.split(":")[1])
+                    traffic = int(line.split(":")[1])
+                if line.startswith("kernel_revision:"):
+                    rev = line.split(":", 1)[1].strip()
     except OSError:
-        pass
-    return None
+        return None, None
+    if traffic is None:
+        return None, None
+    return traffic, f"profiles/{name} (ncu capture at {rev or 'an earlier revision'}; not measured in this run)"
 
 
 def sustain(fn, seconds):
@@ -325,7 +339,9 @@ def cpu_baseline_sample(w, target_s=10.0, threads=1):
         t += time.perf_counter() - t0
         reps += 1
     return {"value": S * reps / t / 1e6, "unit": "Mcells/s", "cores": threads, "kind": "port",
-            "sample": f"first {S} cells of the workload mesh, A+b, {reps} passes, {t:.1f} s"}
+            "sample": (f"first {S} cells of the workload mesh, A+b, {reps} passes, {t:.1f} s; the oracle "
+                       "(CPU restatement of DOLFIN's serial cell loop, element tensors by quadrature), "
+                       "not DOLFIN's own speed")}
 
 
 # ---------------------------------------------------------------------------
@@ -411,6 +427,7 @@ def run_reference(args, rank, world):
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     kind, n, deg, desc = WORKLOADS[args.workload]
+    total_cells = 6 * n ** 3 if kind != "batched" else None
     ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     per = {"elasticity": 512, "poisson": 32768 if deg == 1 else 4096, "batched": 16384}[kind]
     procs, qin, qout = [], [], []
@@ -453,12 +470,170 @@ def run_reference(args, rank, world):
         "cpu_baseline": {"value": round(value, 4), "unit": "Mcells/s", "cores": ncores, "kind": "port",
                          "sample": (f"{cells_per_step} cells per step over {ncores} cores "
                                     + ("(whole member meshes, round-robin)" if kind == "batched"
-                                       else "(disjoint cell ranges)")
-                                    + ", oracle restatement of DOLFIN's serial assemble_cells + "
-                                      "EigenMatrix::add")},
+                                       else f"(disjoint cell ranges, {100.0 * cells_per_step / total_cells:.1f} % "
+                                            f"of the {total_cells} cells)")
+                                    + "; the oracle: a CPU restatement of DOLFIN's serial assemble_cells + "
+                                      "EigenMatrix::add whose element tensors come from Gauss-Jacobi "
+                                      "quadrature (slower than FFC's generated tabulate_tensor), so this "
+                                      "is not DOLFIN's own speed")},
         "e2e": {"value": round(value, 4), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+DEFAULT_WORKLOAD = "elasticity_p2_48"
+# B200 FP64 peak, nominal (no measured FP64 figure exists on this pool):
+# context for the matrix-free action's arithmetic rate only.
+NOMINAL_FP64_TFLOPS = 37.0
+
+
+def action_bytes(C, k_node, gdim, Nv, coeff_dofs, N):
+    """Algorithmic bytes of one matrix-free y = A x: cell->node map, vertex
+    coordinates, coefficient dofs, x read and y written once."""
+    return 4 * k_node * C + 8 * gdim * Nv + 8 * coeff_dofs + 16 * N
+
+
+def action_flops(C, k):
+    """Algorithmic FLOPs of one action: the dense element matrix-vector
+    product, 2 k^2 per cell (k dofs per cell)."""
+    return 2 * k * k * C
+
+
+def dofs_per_cell(w):
+    k_node = 10 if w["deg"] == 2 else 4
+    return k_node * (3 if w["kind"] == "elasticity" else 1)
+
+
+def measure_action(w, args, flush, peak, repeats=0):
+    """Matrix-free action on the workload's form: per-action device time
+    (L2 flushed between actions), the roofline numbers, and optionally the
+    time of `repeats` back-to-back actions (one event window)."""
+    import torch
+    import dolfin_b200 as d2
+    V, mesh = w["V"], w["mesh"]
+    x = torch.randn(V.dim(), dtype=torch.float64, device="cuda",
+                    generator=torch.Generator("cuda").manual_seed(7))
+    xv, y = d2.Vector(x), d2.Vector(n=V.dim())
+    for _ in range(args.warmup):
+        d2.assemble_action(w["a"], xv, y)
+    ms = float(np.mean(time_steps(lambda: d2.assemble_action(w["a"], xv, y), args.steps, flush)))
+    C, Nv = mesh.num_cells(), mesh.num_vertices()
+    k_node = 10 if w["deg"] == 2 else 4
+    by = action_bytes(C, k_node, 3, Nv, Nv if w["kind"] == "poisson" else 0, V.dim())
+    fl = action_flops(C, dofs_per_cell(w))
+    gbs = by / (ms * 1e-3) / 1e9
+    gfs = fl / (ms * 1e-3) / 1e9
+    out = {"ms_per_action": round(ms, 4), "mcells_s": round(C / (ms * 1e-3) / 1e6, 3),
+           "roofline": {"bound": "hbm", "algorithmic_bytes": by, "achieved": round(gbs, 1), "peak": peak,
+                        "unit": "GB/s", "frac": round(gbs / peak, 4),
+                        "algorithmic_flops": fl, "gflops": round(gfs, 1),
+                        "fp64_frac_of_nominal": round(gfs / (NOMINAL_FP64_TFLOPS * 1e3), 4),
+                        "flops_note": "2 k^2 per cell (dense element mat-vec); FP64 peak nominal "
+                                      f"{NOMINAL_FP64_TFLOPS} TFLOP/s, not measured"}}
+    if repeats:
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        s.record()
+        for _ in range(repeats):
+            d2.assemble_action(w["a"], xv, y)
+        e.record()
+        torch.cuda.synchronize()
+        tot = s.elapsed_time(e)
+        out["repeated"] = {"actions": repeats, "ms_total": round(tot, 3),
+                           "ms_per_action": round(tot / repeats, 4),
+                           "frac": round(by / (tot / repeats * 1e-3) / 1e9 / peak, 4)}
+    return out
+
+
+def measure_assembly(w, args, flush, precision="fp64"):
+    """Device time per SystemAssembler step (A and b) at a precision, and
+    the matrix it leaves."""
+    import dolfin_b200 as d2
+    S = w["S"] if precision == "fp64" else d2.SystemAssembler(w["a"], w["L"], precision=precision)
+    A = w["A"] if precision == "fp64" else d2.Matrix(w["V"].pattern())
+    b = w["b"] if precision == "fp64" else d2.Vector(n=w["V"].dim())
+    for _ in range(args.warmup):
+        S.assemble(A, b)
+    ms = float(np.mean(time_steps(lambda: S.assemble(A, b), args.steps, flush)))
+    return ms, A
+
+
+def extra_config5(args, flush, peak, rank):
+    """Scalar P2 Poisson on UnitCubeMesh(96) (5,308,416 cells): FP64 and
+    FP32-contraction A+b steps, their roofline, and 100 repeated matrix-free
+    actions."""
+    import torch
+    w = setup_workload("poisson_p2_96", seed=1000 + rank, device=None)
+    C = w["mesh"].num_cells()
+    ms64, A64 = measure_assembly(w, args, flush, "fp64")
+    v64 = A64.values_tensor().clone()
+    ms32, A32 = measure_assembly(w, args, flush, "fp32")
+    err = float((A32.values_tensor() - v64).abs().max() / v64.abs().max())
+    del A32, v64
+    by = algorithmic_bytes(w)
+    out = {"workload": "poisson_p2_96", "cells": C, "nnz": w["A"].nnz(),
+           "fp64": {"ms_per_step": round(ms64, 4), "mcells_s": round(C / (ms64 * 1e-3) / 1e6, 3),
+                    "roofline_frac": round(by / (ms64 * 1e-3) / 1e9 / peak, 4)},
+           "fp32_contract": {"ms_per_step": round(ms32, 4), "mcells_s": round(C / (ms32 * 1e-3) / 1e6, 3),
+                             "roofline_frac": round(by / (ms32 * 1e-3) / 1e9 / peak, 4),
+                             "speedup_vs_fp64": round(ms64 / ms32, 3), "max_rel_err_vs_fp64": err},
+           "algorithmic_bytes": by, "setup_s": round(w["setup_s"], 2)}
+    out["traffic"], out["traffic_source"] = profiled_traffic("poisson_p2_96")
+    out["matrix_free"] = measure_action(w, args, flush, peak, repeats=100)
+    del w
+    torch.cuda.empty_cache()
+    return out
+
+
+def extra_adjoint(args, flush, rank):
+    """P1 Poisson kappa = exp(g) at n = 64 and 96: the forward A+b step
+    against the adjoint dL/dkappa of L = <gA, A(kappa)> + <gb, b(kappa)>
+    (b = kappa f v dx, whose derivative term the adjoint includes), FP64 and
+    FP32 contraction."""
+    import torch
+    from dolfin_b200.autodiff import vjp_kappa
+    out = {}
+    for name in ("poisson_p1_64", "poisson_p1_96"):
+        w = setup_workload(name, seed=1000 + rank, device=None)
+        ms_fwd, _ = measure_assembly(w, args, flush, "fp64")
+        kt = torch.as_tensor(w["fields"]["kappa"], device="cuda")
+        ft = torch.as_tensor(w["fields"]["f"], device="cuda")
+        g = torch.Generator("cuda").manual_seed(11)
+        gA = torch.randn(w["A"].nnz(), dtype=torch.float64, device="cuda", generator=g)
+        gb = torch.randn(w["V"].dim(), dtype=torch.float64, device="cuda", generator=g)
+        res = {"cells": w["mesh"].num_cells(), "forward_ms": round(ms_fwd, 4)}
+        for prec in ("fp64", "fp32"):
+            fn = lambda: vjp_kappa(w["V"], kt, gA, f=ft, gb=gb, precision=prec)
+            for _ in range(args.warmup):
+                fn()
+            ms = float(np.mean(time_steps(fn, args.steps, flush)))
+            res[f"vjp_{prec}_ms"] = round(ms, 4)
+            res[f"ratio_{prec}_to_forward"] = round(ms / ms_fwd, 3)
+        out[name] = res
+        del w, gA, gb
+        torch.cuda.empty_cache()
+    return out
+
+
+def run_profile(args):
+    """Only the hot loop of one workload (for ncu captures): warm-up plus
+    --steps assembly steps (or matrix-free actions with --profile action),
+    no timing, no JSON line."""
+    import torch
+    import dolfin_b200 as d2
+    w = setup_workload(args.workload, seed=1, device=None, n_override=args.mesh_n)
+    if args.profile == "action":
+        x = torch.randn(w["V"].dim(), dtype=torch.float64, device="cuda",
+                        generator=torch.Generator("cuda").manual_seed(3))
+        xv, y = d2.Vector(x), d2.Vector(n=w["V"].dim())
+        fn = lambda: d2.assemble_action(w["a"], xv, y)
+    else:
+        fn = lambda: w["S"].assemble(w["A"], w["b"])
+    for _ in range(args.warmup + args.steps):
+        fn()
+    torch.cuda.synchronize()
+    print(f"profile {args.workload} n={w['n']} {args.profile}: cells {w['mesh'].num_cells()}, "
+          f"launches {d2.kernel_launches()}", flush=True)
 
 
 def main():
@@ -466,9 +641,14 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="elasticity_p2_48", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the P2 n=96 and adjoint measurements of the default line")
+    ap.add_argument("--profile", choices=["step", "action"], default=None,
+                    help="run only the hot loop (for ncu), print no JSON")
+    ap.add_argument("--mesh-n", type=int, default=None, help="mesh size override (with --profile)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -483,6 +663,9 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.profile:
+        run_profile(args)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -531,43 +714,19 @@ def main():
         ms_step = float(t.item())
     value = cells * world / (ms_step * 1e-3) / 1e6
 
-    # roofline of the dominant kernel (the assembly kernel is the only launch per step)
+    # roofline of the step (the pack kernel and the tile-class launches)
     peak, peak_kind = load_peaks()
     B = algorithmic_bytes(w)
     achieved = B / (ms_step * 1e-3) / 1e9
 
     # FP32 contraction path on the same data
     vals64 = A.values_tensor().clone()
-    b64 = b.tensor().clone()
-    S32 = d2.SystemAssembler(w["a"], w["L"], precision="fp32")
-    A32, b32 = d2.Matrix(w["V"].pattern()), d2.Vector(n=w["V"].dim())
-    S32.assemble(A32, b32)
-    for _ in range(args.warmup):
-        S32.assemble(A32, b32)
-    ms32 = float(np.mean(time_steps(lambda: S32.assemble(A32, b32), args.steps, flush)))
+    ms32, A32 = measure_assembly(w, args, flush, "fp32")
     err32 = float((A32.values_tensor() - vals64).abs().max().item() / vals64.abs().max().item())
+    del A32, vals64
 
     # matrix-free action on the same form
-    x = torch.randn(w["V"].dim(), dtype=torch.float64, device="cuda",
-                    generator=torch.Generator("cuda").manual_seed(7))
-    y = d2.Vector(n=w["V"].dim())
-    for _ in range(args.warmup):
-        d2.assemble_action(w["a"], d2.Vector(x), y)
-    ms_mf = float(np.mean(time_steps(lambda: d2.assemble_action(w["a"], d2.Vector(x), y), args.steps, flush)))
-
-    # adjoint of L(kappa) = <gA, A(kappa)> with respect to the P1 kappa
-    vjp = None
-    if w["kind"] == "poisson":
-        from dolfin_b200.autodiff import vjp_kappa
-        kt = torch.as_tensor(w["fields"]["kappa"], device="cuda")
-        gA = torch.randn(A.nnz(), dtype=torch.float64, device="cuda",
-                         generator=torch.Generator("cuda").manual_seed(11))
-        for _ in range(args.warmup):
-            vjp_kappa(w["V"], kt, gA)
-        ms_vjp = float(np.mean(time_steps(lambda: vjp_kappa(w["V"], kt, gA), args.steps, flush)))
-        vjp = {"ms_per_call": round(ms_vjp, 4), "ratio_to_forward_step": round(ms_vjp / ms_step, 3),
-               "what": "dL/dkappa of L = <gA, A(kappa)>, gA ~ N(0,1) over the CSR values"}
-        del gA
+    mf = measure_action(w, args, flush, peak)
 
     # end to end through the public API with host buffers: per step, H2D of the
     # step's input (vertex coordinates for elasticity, kappa and f otherwise)
@@ -601,32 +760,42 @@ def main():
         e2e_step()
     e2e_ms = (time.perf_counter() - t0) / n_e2e * 1e3
     h2d = sum(t.numel() * 8 for t in h_in)
-    d2h = (nnz + w["V"].dim()) * 8
+    ndofs = w["V"].dim()
+    d2h = (nnz + ndofs) * 8
+    del h_vals, h_b
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(w)
 
+    extras = {}
+    if args.workload == DEFAULT_WORKLOAD and not args.no_extras:
+        del w, S, A, b
+        torch.cuda.empty_cache()
+        extras["config5"] = extra_config5(args, flush, peak, rank)
+        extras["adjoint"] = extra_adjoint(args, flush, rank)
+
     if rank == 0:
         _, n, deg, desc = WORKLOADS[args.workload]
+        traffic, traffic_src = profiled_traffic(args.workload)
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mcells/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded jittered unit-cube mesh; no external dataset)",
             "config": {"workload": args.workload, "description": desc, "cells": cells,
-                       "dofs": w["V"].dim(), "nnz": nnz, "precision": "fp64",
-                       "l2": "flushed between steps (256 MiB write)", "setup_s": round(w["setup_s"], 2),
-                       "parallelism": f"replicas x{world}"},
+                       "dofs": ndofs, "nnz": nnz, "precision": "fp64",
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"replicas x{world}",
+                       "parity": PARITY_NOTE},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": profiled_traffic(args.workload),
+                         "traffic": traffic, "traffic_source": traffic_src,
                          "peak_source": peak_kind, "algorithmic_bytes": B},
             "fp32_contract": {"value": round(cells / (ms32 * 1e-3) / 1e6, 3), "unit": "Mcells/s",
                               "ms_per_step": round(ms32, 4), "speedup_vs_fp64": round(ms_step / ms32, 3),
                               "max_rel_err_vs_fp64": err32},
-            "matrix_free": {"ms_per_action": round(ms_mf, 4),
-                            "mcells_s": round(cells / (ms_mf * 1e-3) / 1e6, 3)},
+            "matrix_free": mf,
             "e2e": {"value": round(cells / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mcells/s",
                     "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -634,8 +803,7 @@ def main():
             "clocks": clk.summary(),
             "wall_s_timed_region": round(t_wall, 3),
         }
-        if vjp is not None:
-            line["vjp"] = vjp
+        line.update(extras)
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
