@@ -20,6 +20,25 @@ def test_library_exports_every_header_symbol():
     assert declared == set(_capi.exported_symbols())
 
 
+def test_cpp_shim_library_loads_and_exports_the_assemblers():
+    """libdolfin_b200_cpp.so (the C++ drop-in classes over the C ABI) loads
+    beside the engine and defines GpuAssembler::assemble and the
+    GpuSystemAssembler entry points declared in dolfin_b200_assembler.h."""
+    import ctypes
+    import subprocess
+    lib = os.path.join(os.path.dirname(__file__), "..", "dolfin_b200", "_lib", "libdolfin_b200_cpp.so")
+    _capi.lib()
+    ctypes.CDLL(lib)
+    syms = subprocess.run(["nm", "-DC", "--defined-only", lib], capture_output=True, text=True,
+                          check=True).stdout
+    for s in ["dolfin_b200::GpuAssembler::assemble(dolfin_b200::GenericTensor&, dolfin_b200::Form const&)",
+              "dolfin_b200::GpuSystemAssembler::assemble(dolfin_b200::Matrix&, dolfin_b200::Vector&)",
+              "dolfin_b200::GpuSystemAssembler::GpuSystemAssembler(",
+              "dolfin_b200::DirichletBC::DirichletBC(",
+              "dolfin_b200::forms::Elasticity("]:
+        assert s in syms, s
+
+
 @pytest.mark.parametrize("n", [(1, 1, 1), (2, 3, 4), (5, 4, 3)])
 def test_unit_cube_mesh(orc, n):
     m = d2.UnitCubeMesh(*n)
