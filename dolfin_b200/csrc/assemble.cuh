@@ -324,6 +324,17 @@ struct Rec {
     const int b = 2 * D + j;
     return (w[b >> 2] >> (8 * (b & 3))) & 0xffu;
   }
+  // Offsets that do not fit 16 bits (vertex numbering spread further than
+  // 32767 within a cell) are stored as -32768: the vertices of such a
+  // record are then read through the incidence word and the cell instead.
+  static constexpr int32_t kEscape = -32768;
+  __device__ __forceinline__ bool escaped(int nused) const {
+    bool e = false;
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+      if (k < nused) e = e || delta(k) == kEscape;
+    return e;
+  }
 };
 
 template <int D, int P>
@@ -359,6 +370,21 @@ __device__ __forceinline__ void relabel(const uint32_t (&v)[D + 1], uint32_t cod
     if constexpr (D == 3) pv[a] = sel4(v, k);
     else pv[a] = sel3(v, k);
   }
+}
+
+template <int D>
+__device__ __forceinline__ void load_verts(const AsmParams& p, uint32_t cell, uint32_t (&v)[D + 1]);
+
+// Relabelled vertex ids of incidence `inc_index` from its incidence word
+// (cell | local node << 28) and the cell's vertex list: the path of records
+// whose offsets did not fit 16 bits.
+template <int D>
+__device__ __noinline__ void incidence_vertices(const AsmParams& p, uint32_t inc_index,
+                                                uint32_t (&pv)[D + 1]) {
+  const uint32_t w = __ldg(p.inc + inc_index);
+  uint32_t v[D + 1];
+  load_verts<D>(p, w & 0x0fffffffu, v);
+  relabel<D>(v, perm_of<D>(int(w >> 28)), pv);
 }
 
 template <int D>
@@ -452,10 +478,14 @@ __device__ __forceinline__ RowFix<D> load_row_fix_n(const AsmParams& p, uint32_t
   return r;
 }
 
-template <int D, int P, bool FP1, int NFIX>
+template <int D, int P, bool FP1, int NFIX, bool ESC>
 __device__ __forceinline__ void record_cell_n(const AsmParams& p, const RowFix<D>& F,
-                                              const Rec<D, P>& r, double (&x)[D + 1][D],
+                                              const Rec<D, P>& r, uint32_t inc_index,
+                                              double (&x)[D + 1][D],
                                               double (&kap)[D + 1], double (&fv)[D + 1]) {
+  uint32_t pv[D + 1] = {};
+  const bool esc = ESC && r.escaped(D + 1 - NFIX);
+  if (esc) incidence_vertices<D>(p, inc_index, pv);
 #pragma unroll
   for (int a = 0; a <= D; ++a) {
     if (a < NFIX) {
@@ -464,7 +494,7 @@ __device__ __forceinline__ void record_cell_n(const AsmParams& p, const RowFix<D
       kap[a] = F.kap[a];
       fv[a] = F.f[a];
     } else {
-      const uint32_t v = uint32_t(int32_t(F.base) + r.delta(a - NFIX));
+      const uint32_t v = esc ? pv[a] : uint32_t(int32_t(F.base) + r.delta(a - NFIX));
       load_vertex<D, FP1>(p, v, x[a], kap[a], fv[a]);
     }
   }
@@ -487,13 +517,19 @@ __device__ __forceinline__ RowFixId load_row_fix_id(const AsmParams& p, uint32_t
   }
   return r;
 }
-template <int D, int P, bool FP1, int NFIX>
+template <int D, int P, bool FP1, int NFIX, bool ESC>
 __device__ __forceinline__ void record_cell_id(const AsmParams& p, const RowFixId& F,
-                                               const Rec<D, P>& r, double (&x)[D + 1][D],
+                                               const Rec<D, P>& r, uint32_t inc_index,
+                                               double (&x)[D + 1][D],
                                                double (&kap)[D + 1], double (&fv)[D + 1]) {
+  uint32_t pv[D + 1] = {};
+  const bool esc = ESC && r.escaped(D + 1 - NFIX);
+  if (esc) incidence_vertices<D>(p, inc_index, pv);
 #pragma unroll
   for (int a = 0; a <= D; ++a) {
-    const uint32_t v = a < NFIX ? F.v[a] : uint32_t(int32_t(F.v[0]) + r.delta(a - NFIX));
+    const uint32_t v = a < NFIX ? F.v[a]
+                       : esc    ? pv[a]
+                                : uint32_t(int32_t(F.v[0]) + r.delta(a - NFIX));
     load_vertex<D, FP1>(p, v, x[a], kap[a], fv[a]);
   }
 }
@@ -501,8 +537,12 @@ __device__ __forceinline__ void record_cell_id(const AsmParams& p, const RowFixI
 // The relabelled cell of one record: fixed vertices first, then the others.
 template <int D, int P, bool FP1>
 __device__ __forceinline__ void record_cell(const AsmParams& p, const RowFix<D>& F,
-                                            const Rec<D, P>& r, double (&x)[D + 1][D],
+                                            const Rec<D, P>& r, uint32_t inc_index,
+                                            double (&x)[D + 1][D],
                                             double (&kap)[D + 1], double (&fv)[D + 1]) {
+  uint32_t pv[D + 1] = {};
+  const bool esc = r.escaped(D + 1 - F.nfix);
+  if (esc) incidence_vertices<D>(p, inc_index, pv);
 #pragma unroll
   for (int a = 0; a <= D; ++a) {
     if (a < F.nfix) {
@@ -511,7 +551,7 @@ __device__ __forceinline__ void record_cell(const AsmParams& p, const RowFix<D>&
       kap[a] = F.kap[a];
       fv[a] = F.f[a];
     } else {
-      const uint32_t v = uint32_t(int32_t(F.base) + r.delta(a - F.nfix));
+      const uint32_t v = esc ? pv[a] : uint32_t(int32_t(F.base) + r.delta(a - F.nfix));
       load_vertex<D, FP1>(p, v, x[a], kap[a], fv[a]);
     }
   }
@@ -603,7 +643,7 @@ __device__ __forceinline__ double load_row(const AsmParams& p, const Geometry<D>
 
 // One row unit (node row, trial block e) of a tile whose rows are all vertex
 // nodes (NFIX = 1 fixed vertex) or all edge nodes (NFIX = 2).
-template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int NFIX>
+template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int NFIX, bool ESC>
 __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, double* acc,
                                          double* bpart, int32_t r0, int u) {
   using E = El<D, P>;
@@ -616,7 +656,8 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
   const int32_t ra = __ldg(p.node_rowptr + node);
   const int32_t L = __ldg(p.node_rowptr + node + 1) - ra;
   double* my = acc + BS * (ra - r0) + e * L;
-  const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - __ldg(p.inc_ptr + node);
+  const uint32_t i0 = __ldg(p.inc_ptr + node);
+  const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - i0;
   const uint32_t rbase = __ldg(p.rec_goff + (node >> 5)) + (node & 31u);
   double bsum = 0.0;
   const int64_t rowdof = int64_t(t.comp) * p.nnodes + node;
@@ -671,8 +712,8 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
     const Rec<D, P> r = rn;
     if (m + 1 < cnt) rn = load_rec<D, P>(p, rbase + 32u * (m + 1));
     double x[D + 1][D], kap[D + 1], fv[D + 1];
-    if constexpr (RELOAD) record_cell_id<D, P, FP1, NFIX>(p, F, r, x, kap, fv);
-    else record_cell_n<D, P, FP1, NFIX>(p, F, r, x, kap, fv);
+    if constexpr (RELOAD) record_cell_id<D, P, FP1, NFIX, ESC>(p, F, r, i0 + m, x, kap, fv);
+    else record_cell_n<D, P, FP1, NFIX, ESC>(p, F, r, i0 + m, x, kap, fv);
     Geometry<D> G;
     geometry(x, G);
     CT out[E::K];
@@ -736,7 +777,7 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
 // per cell: a Dirichlet row keeps only 1 on its diagonal and contributes g_i
 // to b; other rows move their Dirichlet-column entries to b (b_i -= A_ij g_j)
 // and zero them.
-template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
+template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, bool ESC = false>
 __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, double* acc) {
   constexpr int BS = FORM == FORM_ELAS ? D : 1;
   const int32_t r0 = __ldg(p.node_rowptr + t.n0), r1 = __ldg(p.node_rowptr + t.n1);
@@ -747,9 +788,9 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
     // tiles never mix vertex and edge nodes (the host cuts P2 tiles at the
     // first edge node), so the row kind is uniform over the block
     if (P == 1 || t.n0 < p.nverts)
-      row_unit<D, P, FORM, KP1, LOADM, CT, 1>(p, t, acc, bpart, r0, int(threadIdx.x));
+      row_unit<D, P, FORM, KP1, LOADM, CT, 1, ESC>(p, t, acc, bpart, r0, int(threadIdx.x));
     else if constexpr (P == 2)
-      row_unit<D, P, FORM, KP1, LOADM, CT, 2>(p, t, acc, bpart, r0, int(threadIdx.x));
+      row_unit<D, P, FORM, KP1, LOADM, CT, 2, ESC>(p, t, acc, bpart, r0, int(threadIdx.x));
   }
   __syncthreads();
   if constexpr (LOADM != LOAD_NONE) {
@@ -802,10 +843,12 @@ constexpr int tile_maxnreg() {
          : P == 1            ? DB2_TILE_MAXNREG_P1
                              : DB2_TILE_MAXNREG_P2;
 }
-template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
+// ESC: the pattern has records whose vertex offsets did not fit 16 bits
+// (a separate instantiation, so that well-numbered meshes pay nothing).
+template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, bool ESC>
 __global__ void __maxnreg__((tile_maxnreg<P, FORM, CT>())) k_assemble(const AsmParams p) {
   extern __shared__ double acc[];
-  tile_body<D, P, FORM, KP1, LOADM, CT>(p, p.tiles[blockIdx.x], acc);
+  tile_body<D, P, FORM, KP1, LOADM, CT, ESC>(p, p.tiles[blockIdx.x], acc);
 }
 
 }  // namespace dev

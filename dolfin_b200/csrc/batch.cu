@@ -193,6 +193,10 @@ int db2_batch_create(int count, const db2_pattern* patterns, const db2_form* for
           fail(DB2_ERR_UNSUPPORTED, "batch member %d: only kappa*grad.grad with a P1 kappa", m);
         if (!kappas[m] || !vals[m]) fail(DB2_ERR_ARGUMENT, "batch member %d: NULL kappa/vals", m);
         P->ensure_device();
+        if (P->rec_escapes)
+          fail(DB2_ERR_UNSUPPORTED,
+               "batch member %d: cell vertex ids more than 32767 apart (assemble it on its own, "
+               "which handles any numbering)", m);
         B.patterns.push_back(P);
         dev::BatchMember bm{};
         bm.p = make_params(*P);

@@ -695,7 +695,7 @@ void Pattern::ensure_device() {
     }
     std::vector<uint8_t> rec(size_t(rec_goff[ngrp]) * rs, 0);
     std::vector<uint8_t> first(size_t(nn) * rs, 0);
-    std::atomic<int64_t> bad{-1};
+    std::atomic<int64_t> escapes{0};
     parallel_for(nn, [&](int64_t b, int64_t e) {
       for (int64_t i = b; i < e; ++i) {
         // edge-node rows: which of the record's slots this incidence is the
@@ -712,8 +712,11 @@ void Pattern::ensure_device() {
           uint8_t* r = &rec[(size_t(rec_goff[i >> 5]) + (i & 31) + 32ull * (s - inc_ptr[i])) * rs];
           for (int a = nfix; a <= D; ++a) {
             const int64_t d = int64_t(cv[perm[a]]) - base;
-            if (d < -32768 || d > 32767) bad = i;
-            const int16_t d16 = int16_t(d);
+            // -32768 marks an offset that does not fit: the kernel then
+            // reads this incidence's vertices through its cell
+            const bool fits = d >= -32767 && d <= 32767;
+            if (!fits) escapes.fetch_add(1, std::memory_order_relaxed);
+            const int16_t d16 = fits ? int16_t(d) : int16_t(-32768);
             std::memcpy(r + 2 * (a - nfix), &d16, 2);
           }
           std::memcpy(r + 2 * nd, &pos[size_t(s) * kp], size_t(K));
@@ -732,9 +735,7 @@ void Pattern::ensure_device() {
         }
       }
     });
-    if (bad >= 0)
-      fail(DB2_ERR_UNSUPPORTED, "vertex numbering too spread for 16-bit cell offsets (node %lld); "
-           "renumber the mesh vertices for locality", (long long)bad.load());
+    rec_escapes = escapes.load();
     d_rec.upload(rec.data(), rec.size());
     d_rec_goff.upload(rec_goff.data(), rec_goff.size() * sizeof(uint32_t));
     d_rec_first.upload(first.data(), first.size());

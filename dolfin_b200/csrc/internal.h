@@ -146,6 +146,9 @@ struct Pattern {
   // each block of 32 consecutive nodes are interleaved (record m of node i at
   // rec_goff[i/32] + i%32 + 32 m) so that a warp's loads are contiguous.
   int rs = 8;
+  // records whose offsets did not fit 16 bits (stored as -32768; the kernel
+  // then reads the cell's vertices through the incidence word)
+  int64_t rec_escapes = 0;
   std::vector<uint32_t> rec_goff;    // per 32-node block: first record index
   DeviceBuffer d_node_rowptr, d_inc_ptr, d_inc, d_rec, d_rec_goff, d_cell_inc, d_tiles, d_rowptr, d_cols;
   // each node's first record again, node-indexed: the row walk's first

@@ -16,13 +16,14 @@ __global__ void __launch_bounds__(256) k_assemble_vector(const AsmParams p, int 
   const int c = int(r / p.nnodes);
   const int64_t node = r - int64_t(c) * p.nnodes;
   double bsum = 0.0;
-  const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - __ldg(p.inc_ptr + node);
+  const uint32_t i0 = __ldg(p.inc_ptr + node);
+  const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - i0;
   const uint32_t rbase = __ldg(p.rec_goff + (node >> 5)) + uint32_t(node & 31);
   const RowFix<D> F = load_row_fix<D, P, LOADM == LOAD_P1>(p, uint32_t(node));
   for (uint32_t m = 0; m < cnt; ++m) {
     const Rec<D, P> r = load_rec<D, P>(p, rbase + 32u * m);
     double x[D + 1][D], kap[D + 1], fv[D + 1];
-    record_cell<D, P, LOADM == LOAD_P1>(p, F, r, x, kap, fv);
+    record_cell<D, P, LOADM == LOAD_P1>(p, F, r, i0 + m, x, kap, fv);
     Geometry<D> G;
     geometry(x, G);
     bsum += load_row<D, P, LOADM>(p, G, F.nfix == 1, c, fv);
@@ -160,6 +161,7 @@ void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int
   cfg.class_smem = &P.class_smem;
   cfg.threads = P.tile_threads;
   cfg.stream = static_cast<cudaStream_t>(stream);
+  cfg.escapes = P.rec_escapes > 0;
   const bool fp32 = precision == DB2_FP32_CONTRACT;
   if (precision != DB2_FP64 && precision != DB2_FP32_CONTRACT) fail(DB2_ERR_ARGUMENT, "unknown precision %d", precision);
   bool ok = false;

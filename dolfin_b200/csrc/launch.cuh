@@ -13,6 +13,7 @@ struct LaunchCfg {
   const std::vector<int32_t>* class_smem;
   int threads;
   cudaStream_t stream;
+  bool escapes = false;  // the pattern has records with escaped vertex offsets
 };
 
 // Let `kern` use all the dynamic shared memory the current device allows a
@@ -70,9 +71,10 @@ inline SideStreams& side_streams() {
 // alone below the SM's residency limits.
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
 void run_assemble(const AsmParams& p, const LaunchCfg& cfg) {
-  auto kern = k_assemble<D, P, FORM, KP1, LOADM, CT>;
-  static unsigned long long configured = 0;
-  allow_dynamic_smem(kern, configured);
+  auto kern = cfg.escapes ? k_assemble<D, P, FORM, KP1, LOADM, CT, true>
+                          : k_assemble<D, P, FORM, KP1, LOADM, CT, false>;
+  static unsigned long long configured[2] = {0, 0};
+  allow_dynamic_smem(kern, configured[cfg.escapes ? 1 : 0]);
   const auto& cb = *cfg.class_begin;
   const int ncls = int(cb.size()) - 1;
   const bool fork = DB2_CLASS_STREAMS && ncls > 1 && ncls <= SideStreams::kMax;

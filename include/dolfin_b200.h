@@ -163,7 +163,14 @@ int db2_space_destroy(db2_space V);
 /* SparsityPatternBuilder::build (dolfin/fem/SparsityPatternBuilder.cpp:42-269)
    + EigenMatrix::init (dolfin/la/EigenMatrix.cpp:384-410) for a on V x V:
    sorted CSR (int32 rowptr/cols, as Eigen::SparseMatrix<double,RowMajor,int>),
-   plus the engine's row-gather plan.  keep_diagonal as AssemblerBase.h:67. */
+   plus the engine's row-gather plan.  keep_diagonal as AssemblerBase.h:67.
+   Limits of the plan (DB2_ERR_UNSUPPORTED beyond them): fewer than 2^28
+   cells (an incidence word holds the cell in 28 bits), at most 255 distinct
+   nodes in a node's row (column slots are bytes), nnz and the global
+   dimension within int32 (Eigen's StorageIndex).  Any vertex numbering is
+   accepted: incidences whose cell spans more than 32767 vertex ids (16-bit
+   offsets in the plan's records) read their cell's vertex list instead,
+   which costs two dependent loads on those incidences only. */
 int db2_pattern_create(db2_space V, int keep_diagonal, db2_pattern* out);
 int db2_pattern_info(db2_pattern P, int64_t* nrows, int64_t* nnz);
 /* Device CSR arrays owned by the pattern (EigenMatrix::data(),
