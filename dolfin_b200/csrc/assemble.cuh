@@ -641,14 +641,9 @@ __device__ __forceinline__ double load_row(const AsmParams& p, const Geometry<D>
 }
 
 
-// One row unit of a tile whose rows are all vertex nodes (NFIX = 1 fixed
-// vertex) or all edge nodes (NFIX = 2): the node row of test component
-// t.comp.  Scalar forms: unit u = node u of the tile.  Elasticity: every
-// tile holds one (test component CC, trial component EE) block, fixed at
-// compile time (no runtime component selects in the element row); unit u =
-// node u, whose block occupies its L slots of the tile segment.
-template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int NFIX, bool ESC,
-          int CC = 0, int EE = 0>
+// One row unit (node row, trial block e) of a tile whose rows are all vertex
+// nodes (NFIX = 1 fixed vertex) or all edge nodes (NFIX = 2).
+template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int NFIX, bool ESC>
 __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, double* acc,
                                          double* bpart, int32_t r0, int u) {
   using E = El<D, P>;
@@ -656,24 +651,23 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
   constexpr bool FP1 = LOADM == LOAD_P1;
   constexpr bool vertex = NFIX == 1;
   const bool bc = p.bc_flags != nullptr;
-  const uint32_t node = t.n0 + u;
-  constexpr int e = EE;
+  const uint32_t node = t.n0 + u / BS;
+  const int e = u % BS;
   const int32_t ra = __ldg(p.node_rowptr + node);
   const int32_t L = __ldg(p.node_rowptr + node + 1) - ra;
-  double* my = acc + (ra - r0);
+  double* my = acc + BS * (ra - r0) + e * L;
   const uint32_t i0 = __ldg(p.inc_ptr + node);
   const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - i0;
   const uint32_t rbase = __ldg(p.rec_goff + (node >> 5)) + (node & 31u);
   double bsum = 0.0;
-  const int comp = FORM == FORM_ELAS ? CC : t.comp;
-  const int64_t rowdof = int64_t(comp) * p.nnodes + node;
+  const int64_t rowdof = int64_t(t.comp) * p.nnodes + node;
   bool row_bc = false;
   double row_g = 0.0;
   const int32_t* colrow = nullptr;
   if (bc) {
     row_bc = __ldg(p.bc_flags + rowdof) != 0;
     row_g = row_bc ? __ldg(p.bc_vals + rowdof) : 0.0;
-    colrow = p.cols + int64_t(comp) * BS * p.nnz_node + int64_t(BS) * ra + e * L;
+    colrow = p.cols + int64_t(t.comp) * BS * p.nnz_node + int64_t(BS) * ra + e * L;
   }
   // Elasticity rows reload their fixed vertices with every incidence (L1
   // hits); the Poisson rows keep them in registers (measured on B200:
@@ -723,16 +717,16 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
     Geometry<D> G;
     geometry(x, G);
     CT out[E::K];
-    element_row<D, P, FORM, KP1, CT>(p, G, vertex, comp, e, kap, out);
+    element_row<D, P, FORM, KP1, CT>(p, G, vertex, t.comp, e, kap, out);
     if constexpr (LOADM != LOAD_NONE) {
-      if (e == 0) bsum += load_row<D, P, LOADM>(p, G, vertex, comp, fv);
+      if (e == 0) bsum += load_row<D, P, LOADM>(p, G, vertex, t.comp, fv);
     }
     if (bc) {
       if (row_bc) {
 #pragma unroll
-        for (int j = 0; j < E::K; ++j) out[j] = CT((e == comp && j == jstar) ? 1 : 0);
+        for (int j = 0; j < E::K; ++j) out[j] = CT((e == t.comp && j == jstar) ? 1 : 0);
         if constexpr (LOADM != LOAD_NONE) {
-          if (e == 0) bsum = bsum - load_row<D, P, LOADM>(p, G, vertex, comp, fv) + row_g;
+          if (e == 0) bsum = bsum - load_row<D, P, LOADM>(p, G, vertex, t.comp, fv) + row_g;
         }
       } else {
 #pragma unroll
@@ -774,81 +768,46 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
   bpart[u] = bsum;
 }
 
-// One tile: rows [t.n0, t.n1) of test component t.comp (and, for
-// elasticity, trial block t.pad).  `acc` holds the tile's CSR value segment
-// (the nodes' rows -- for elasticity the tile's block of each node row --
-// one after another) followed by one double per row unit (load-vector
-// partials).  blockDim must be at least the tile's node count.
+// One tile: rows [t.n0, t.n1) of test component t.comp.  `acc` holds the
+// tile's CSR value segment followed by one double per row unit (load-vector
+// partials).  blockDim must be at least the tile's unit count.
 //
 // With Dirichlet data (p.bc_flags) each element row is modified as
 // SystemAssembler::apply_bc (dolfin/fem/SystemAssembler.cpp:1037-1070) does
 // per cell: a Dirichlet row keeps only 1 on its diagonal and contributes g_i
 // to b; other rows move their Dirichlet-column entries to b (b_i -= A_ij g_j)
 // and zero them.
-template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, bool ESC, int CC, int EE>
-__device__ __forceinline__ void tile_rows(const AsmParams& p, const Tile& t, double* acc,
-                                          double* bpart, int32_t r0) {
-  if (int(threadIdx.x) < t.n1 - t.n0) {
-    // tiles never mix vertex and edge nodes (the host cuts P2 tiles at the
-    // first edge node), so the row kind is uniform over the block
-    if (P == 1 || t.n0 < p.nverts)
-      row_unit<D, P, FORM, KP1, LOADM, CT, 1, ESC, CC, EE>(p, t, acc, bpart, r0, int(threadIdx.x));
-    else if constexpr (P == 2)
-      row_unit<D, P, FORM, KP1, LOADM, CT, 2, ESC, CC, EE>(p, t, acc, bpart, r0, int(threadIdx.x));
-  }
-}
-
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, bool ESC = false>
 __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, double* acc) {
   constexpr int BS = FORM == FORM_ELAS ? D : 1;
   const int32_t r0 = __ldg(p.node_rowptr + t.n0), r1 = __ldg(p.node_rowptr + t.n1);
-  const int seg = r1 - r0;
+  const int seg = BS * (r1 - r0);
   double* bpart = acc + seg;
-  if constexpr (FORM == FORM_ELAS) {
-    // block-uniform dispatch to the tile's (test, trial) component pair
-    switch (t.comp * 3 + t.pad) {
-#define DB2_CE(C_, E_) \
-      case C_ * 3 + E_: tile_rows<D, P, FORM, KP1, LOADM, CT, ESC, C_, E_>(p, t, acc, bpart, r0); break;
-      DB2_CE(0, 0) DB2_CE(0, 1) DB2_CE(0, 2) DB2_CE(1, 0) DB2_CE(1, 1) DB2_CE(1, 2)
-      DB2_CE(2, 0) DB2_CE(2, 1) DB2_CE(2, 2)
-#undef DB2_CE
-      default: break;
-    }
-  } else {
-    tile_rows<D, P, FORM, KP1, LOADM, CT, ESC, 0, 0>(p, t, acc, bpart, r0);
+  const int units = (t.n1 - t.n0) * BS;
+  if (int(threadIdx.x) < units) {
+    // tiles never mix vertex and edge nodes (the host cuts P2 tiles at the
+    // first edge node), so the row kind is uniform over the block
+    if (P == 1 || t.n0 < p.nverts)
+      row_unit<D, P, FORM, KP1, LOADM, CT, 1, ESC>(p, t, acc, bpart, r0, int(threadIdx.x));
+    else if constexpr (P == 2)
+      row_unit<D, P, FORM, KP1, LOADM, CT, 2, ESC>(p, t, acc, bpart, r0, int(threadIdx.x));
   }
   __syncthreads();
   if constexpr (LOADM != LOAD_NONE) {
-    // b of each row (elasticity: the trial-block-0 tile of the row's nodes)
-    if (FORM != FORM_ELAS || t.pad == 0)
-      for (int i = threadIdx.x; i < t.n1 - t.n0; i += blockDim.x) {
-        double* bp = p.b + int64_t(t.comp) * p.nnodes + t.n0 + i;
-        *bp = p.add_values ? *bp + bpart[i] : bpart[i];
-      }
+    // b of each row: its trial blocks' partials in block order
+    for (int i = threadIdx.x; i < t.n1 - t.n0; i += blockDim.x) {
+      double s = 0.0;
+#pragma unroll
+      for (int e = 0; e < BS; ++e) s += bpart[i * BS + e];
+      double* bp = p.b + int64_t(t.comp) * p.nnodes + t.n0 + i;
+      *bp = p.add_values ? *bp + s : s;
+    }
   }
-  if constexpr (FORM == FORM_ELAS) {
-    // node i's block goes to row (comp, node) at trial block t.pad: one
-    // contiguous run per node, written by the whole block
-    double* dst = p.vals + int64_t(t.comp) * BS * p.nnz_node;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int i = warp; i < t.n1 - t.n0; i += nw) {
-      const int32_t ra = __ldg(p.node_rowptr + t.n0 + i);
-      const int32_t L = __ldg(p.node_rowptr + t.n0 + i + 1) - ra;
-      double* d = dst + int64_t(BS) * ra + int64_t(t.pad) * L;
-      const double* a = acc + (ra - r0);
-      if (p.add_values) {
-        for (int k = lane; k < L; k += 32) d[k] += a[k];
-      } else {
-        for (int k = lane; k < L; k += 32) d[k] = a[k];
-      }
-    }
+  double* dst = p.vals + int64_t(t.comp) * BS * p.nnz_node + int64_t(BS) * r0;
+  if (p.add_values) {
+    for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] += acc[i];
   } else {
-    double* dst = p.vals + int64_t(t.comp) * p.nnz_node + r0;
-    if (p.add_values) {
-      for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] += acc[i];
-    } else {
-      for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] = acc[i];
-    }
+    for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] = acc[i];
   }
   __syncthreads();
 }

@@ -471,12 +471,9 @@ void canonical_node_map(int tdim, int degree, int li, int* map) {
 // incident cells in ascending order -- the order in which DOLFIN's cell loop
 // adds their contributions to row i.
 // ---------------------------------------------------------------------------
-// Tiles: contiguous node ranges with at most one row unit (node) per thread
-// whose row segment fits seg_cap_doubles.  Vector spaces (elasticity) get
-// one tile per (test component c, trial component e) of each node range --
-// Tile::pad holds e -- so both components are fixed per CTA; the nine tiles
-// of a node range are consecutive, so they find its incidence records and
-// vertices in L2.
+// Tiles: contiguous node ranges with at most one row unit (node x trial
+// block) per thread whose row segment (one test component) fits
+// seg_cap_doubles.
 
 std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doubles, int* max_seg_out,
                             int64_t node_begin, int64_t node_end) {
@@ -486,32 +483,34 @@ std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doub
   // kernel knows each tile's row kind up front
   const int64_t split = P.V->degree == 2 ? P.V->mesh->nv : -1;
   int max_seg = 0;
-  std::vector<Tile> ranges;
+  std::vector<Tile> comp0;
   int64_t n0 = node_begin;
   while (n0 < nn) {
     int64_t n1 = n0;
     while (n1 < nn) {
       if (n1 == split && n1 > n0) break;
-      const int64_t units = n1 + 1 - n0;
-      const int64_t seg = P.node_rowptr[n1 + 1] - P.node_rowptr[n0];
+      const int64_t units = (n1 + 1 - n0) * bs;
+      const int64_t seg = int64_t(bs) * (P.node_rowptr[n1 + 1] - P.node_rowptr[n0]);
       if (units > tile_threads || seg > seg_cap_doubles) break;
       ++n1;
     }
     if (n1 == n0) fail(DB2_ERR_UNSUPPORTED, "row of node %lld does not fit one tile", (long long)n0);
-    max_seg = std::max<int>(max_seg, int(P.node_rowptr[n1] - P.node_rowptr[n0]));
-    ranges.push_back(Tile{0, int32_t(n0), int32_t(n1), 0});
+    max_seg = std::max<int>(max_seg, int(int64_t(bs) * (P.node_rowptr[n1] - P.node_rowptr[n0])));
+    comp0.push_back(Tile{0, int32_t(n0), int32_t(n1), 0});
     n0 = n1;
   }
   std::vector<Tile> all;
-  all.reserve(ranges.size() * bs * bs);
-  for (const Tile& r : ranges)
-    for (int c = 0; c < bs; ++c)
-      for (int e = 0; e < bs; ++e) all.push_back(Tile{c, r.n0, r.n1, e});
+  for (int c = 0; c < bs; ++c)
+    for (auto t : comp0) {
+      t.comp = c;
+      all.push_back(t);
+    }
   if (max_seg_out) *max_seg_out = max_seg;
   return all;
 }
 
 static void build_tiles(Pattern& P, int tile_threads, int seg_cap_doubles) {
+  const int bs = P.bs;
   P.tile_threads = tile_threads;
   P.seg_cap_bytes = seg_cap_doubles * 8;
   int max_seg = 0;
@@ -524,7 +523,7 @@ static void build_tiles(Pattern& P, int tile_threads, int seg_cap_doubles) {
                                98304, 131072, 163840, 196608, 227 * 1024};
   const int ncls = int(sizeof(kClass) / sizeof(kClass[0]));
   auto cls_of = [&](const Tile& t) {
-    const int64_t need = int64_t(P.node_rowptr[t.n1] - P.node_rowptr[t.n0]) * 8;
+    const int64_t need = int64_t(bs) * (P.node_rowptr[t.n1] - P.node_rowptr[t.n0]) * 8;
     int k = 0;
     while (k < ncls - 1 && kClass[k] < need) ++k;
     return k;

@@ -115,15 +115,13 @@ def test_tiles_cover_rows_once():
     V = d2.VectorFunctionSpace(m, "Lagrange", 2)
     plan = V.pattern().plan()
     t = plan["tiles"]
-    t = t[np.lexsort((t[:, 1], t[:, 3], t[:, 0]))]
+    t = t[np.lexsort((t[:, 1], t[:, 0]))]
     nn = V.dim() // 3
-    # one tile per (test component, trial component) of every node range
     for c in range(3):
-        for e in range(3):
-            tc = t[(t[:, 0] == c) & (t[:, 3] == e)]
-            assert tc[0, 1] == 0 and tc[-1, 2] == nn
-            assert np.all(tc[1:, 1] == tc[:-1, 2])
-            assert np.all(tc[:, 2] > tc[:, 1])
+        tc = t[t[:, 0] == c]
+        assert tc[0, 1] == 0 and tc[-1, 2] == nn
+        assert np.all(tc[1:, 1] == tc[:-1, 2])
+        assert np.all(tc[:, 2] > tc[:, 1])
 
 
 def test_errors_are_raised_not_crashed():
@@ -288,11 +286,9 @@ def test_row_range_tiles_cover_exactly_the_range():
         P.set_row_range(a, b)
         t = P.plan()["tiles"]
         for c in range(3):
-            for e in range(3):
-                tc = t[(t[:, 0] == c) & (t[:, 3] == e)]
-                covered = (np.concatenate([np.arange(n0, n1) for _, n0, n1, _ in tc]) if len(tc)
-                           else np.array([], int))
-                assert np.array_equal(np.sort(covered), np.arange(a, b))
+            tc = t[t[:, 0] == c]
+            covered = np.concatenate([np.arange(n0, n1) for _, n0, n1, _ in tc]) if len(tc) else np.array([], int)
+            assert np.array_equal(np.sort(covered), np.arange(a, b))
     P.set_row_range(0, nn)
     assert len(P.plan()["tiles"]) > 0
     for a, b in [(-1, 3), (5, 4), (0, nn + 1)]:
