@@ -36,9 +36,9 @@ WORKLOADS = {
     "elasticity_p2_48": ("elasticity", 48, 2, "vector P2 elasticity, UnitCubeMesh(48) jittered 0.15h, A+b"),
     "poisson_p1_32": ("poisson", 32, 1, "P1 Poisson kappa P1 + load f P1, UnitCubeMesh(32), A+b"),
     "poisson_p2_96": ("poisson", 96, 2, "P2 Poisson kappa P1 + load f P1, UnitCubeMesh(96), A+b"),
-    "poisson_p1_64": ("poisson", 64, 1, "P1 Poisson kappa=exp(g) g~N(0,0.25) + load f P1, "
+    "poisson_p1_64": ("poisson", 64, 1, "P1 Poisson kappa=exp(g) g~N(0,0.25) + load kappa*f (f P1), "
                       "UnitCubeMesh(64), A+b; adjoint dL/dkappa timed beside it"),
-    "poisson_p1_96": ("poisson", 96, 1, "P1 Poisson kappa=exp(g) g~N(0,0.25) + load f P1, "
+    "poisson_p1_96": ("poisson", 96, 1, "P1 Poisson kappa=exp(g) g~N(0,0.25) + load kappa*f (f P1), "
                       "UnitCubeMesh(96), A+b; adjoint dL/dkappa timed beside it"),
     "batched_512": ("batched", 512, 0, "512 UnitSquareMesh(n), n log-uniform [8,256], jitter 0.2h, "
                     "P1/P2 kappa*grad.grad, one graph-captured persistent launch"),
@@ -222,7 +222,7 @@ def setup_workload(name, seed, device, n_override=None):
         sigma = lambda w: 2 * mu * eps(w) + lmbda * d2.tr(eps(w)) * d2.Identity(3)
         a = d2.inner(sigma(u), eps(v)) * d2.dx
         L = d2.inner(d2.Constant((0.0, 0.0, -1.0)), v) * d2.dx
-        fields = {}
+        fields, funcs = {}, ()
     else:
         x = x0
         V = d2.FunctionSpace(mesh, "Lagrange", deg)
@@ -235,15 +235,17 @@ def setup_workload(name, seed, device, n_override=None):
         kappa, f = d2.Function(W, kv), d2.Function(W, fv)
         u, v = d2.TrialFunction(V), d2.TestFunction(V)
         a = kappa * d2.inner(d2.grad(u), d2.grad(v)) * d2.dx
-        L = f * v * d2.dx
+        # the adjoint workloads differentiate A and b: b = kappa*f*v*dx
+        L = (kappa * f * v * d2.dx) if name in LOGNORMAL_KAPPA else (f * v * d2.dx)
         fields = {"kappa": kv, "f": fv}
+        funcs = (kappa, f)
     S = d2.SystemAssembler(a, L)
     A, b = d2.Matrix(), d2.Vector(n=V.dim())
     S.assemble(A, b)  # builds the pattern and the plan, first assembly
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
     return dict(mesh=mesh, V=V, a=a, L=L, S=S, A=A, b=b, x=x, fields=fields, kind=kind, n=n,
-                deg=deg, setup_s=setup_s)
+                deg=deg, setup_s=setup_s, name=name, funcs=funcs)
 
 
 def csr_bytes(nnz, N, C, k_node, gdim, Nv, coeff_dofs, with_b):
@@ -326,16 +328,21 @@ def cpu_baseline_sample(w, target_s=10.0, threads=1):
     if w["kind"] == "elasticity":
         fa = orc.form(orc.ELASTICITY, 3, deg, 3, mu=1 / 2.6, lmbda=0.3 / (1.3 * 0.4))
         fl = orc.form(orc.LOAD, 3, deg, 3, coeff=orc.COEFF_CONST, c=(0, 0, -1))
-        wa = wl = None
+        wa = wl = wl2 = None
     else:
         fa = orc.form(orc.DIFFUSION, 3, deg, 1, coeff=orc.COEFF_P1)
-        fl = orc.form(orc.LOAD, 3, deg, 1, coeff=orc.COEFF_P1)
         wa, wl = w["fields"]["kappa"], w["fields"]["f"]
+        if w["name"] in LOGNORMAL_KAPPA:
+            fl = orc.form(orc.LOAD, 3, deg, 1, coeff=orc.COEFF_P1_TIMES_P1)
+            wl, wl2 = wa, wl
+        else:
+            fl = orc.form(orc.LOAD, 3, deg, 1, coeff=orc.COEFF_P1)
+            wl2 = None
     reps, t = 0, 0.0
     while t < target_s:
         t0 = time.perf_counter()
         orc.assemble_matrix(fa, sub, dsub, dsub, rp, cols, w=wa)
-        orc.assemble_vector(fl, sub, dsub, N, w=wl)
+        orc.assemble_vector(fl, sub, dsub, N, w=wl, w2=wl2)
         t += time.perf_counter() - t0
         reps += 1
     return {"value": S * reps / t / 1e6, "unit": "Mcells/s", "cores": threads, "kind": "port",
@@ -383,19 +390,24 @@ def _ref_init(workload, rank, ncells, ncores):
         om.coords = synthetic.jitter_interior(om.coords, n, 0.15, 1000)
         fa = orc.form(orc.ELASTICITY, 3, deg, 3, mu=1 / 2.6, lmbda=0.3 / (1.3 * 0.4))
         fl = orc.form(orc.LOAD, 3, deg, 3, coeff=orc.COEFF_CONST, c=(0, 0, -1))
-        wa = wl = None
+        wa = wl = wl2 = None
     else:
         fa = orc.form(orc.DIFFUSION, 3, deg, 1, coeff=orc.COEFF_P1)
-        fl = orc.form(orc.LOAD, 3, deg, 1, coeff=orc.COEFF_P1)
         wa = (synthetic.lognormal_field(om.nv, 0.5, 1000) if workload in LOGNORMAL_KAPPA
               else synthetic.uniform_field(om.nv, 0.5, 2.0, 1000))
         wl = synthetic.uniform_field(om.nv, -1.0, 1.0, 1001)
+        if workload in LOGNORMAL_KAPPA:  # b = kappa*f*v*dx
+            fl = orc.form(orc.LOAD, 3, deg, 1, coeff=orc.COEFF_P1_TIMES_P1)
+            wl2, wl = wl, wa
+        else:
+            fl = orc.form(orc.LOAD, 3, deg, 1, coeff=orc.COEFF_P1)
+            wl2 = None
     od, N = orc.dofmap(om, deg, vs)
     lo = (rank * ncells) % om.nc
     sub = orc.Mesh(3, om.coords, np.ascontiguousarray(om.cells[lo:lo + ncells]))
     dsub = np.ascontiguousarray(od[lo:lo + ncells])
     rp, cols = orc.sparsity(N, N, dsub, dsub)
-    _REF.update(orc=orc, sub=sub, dsub=dsub, rp=rp, cols=cols, fa=fa, fl=fl, wa=wa, wl=wl, N=N,
+    _REF.update(orc=orc, sub=sub, dsub=dsub, rp=rp, cols=cols, fa=fa, fl=fl, wa=wa, wl=wl, wl2=wl2, N=N,
                 jobs=None, ncells=sub.nc)
 
 
@@ -407,7 +419,7 @@ def _ref_work(_):
             r["orc"].assemble_matrix(fa, om, od, od, rp, cols, w=kv)
     else:
         r["orc"].assemble_matrix(r["fa"], r["sub"], r["dsub"], r["dsub"], r["rp"], r["cols"], w=r["wa"])
-        r["orc"].assemble_vector(r["fl"], r["sub"], r["dsub"], r["N"], w=r["wl"])
+        r["orc"].assemble_vector(r["fl"], r["sub"], r["dsub"], r["N"], w=r["wl"], w2=r["wl2"])
     return time.perf_counter() - t0
 
 
@@ -615,6 +627,89 @@ def extra_adjoint(args, flush, rank):
     return out
 
 
+def run_split_rows(args, rank, world, local, dist):
+    """One mesh over all ranks: rank r assembles and holds only the CSR rows
+    (and b entries) of its node range -- shard.row_partition cuts the rows
+    at equal incidence counts, shard.RowBlock allocates the block alone.  No
+    data-path collective (row owners compute their rows from the cells
+    around them); the time is the max over ranks (strong scaling)."""
+    import torch
+    from dolfin_b200 import _capi, shard
+    if WORKLOADS[args.workload][0] == "batched":
+        raise SystemExit("--split rows is for single-mesh workloads (the batched one is split by mesh)")
+    w = setup_workload(args.workload, seed=1000, device=local)  # the same mesh on every rank
+    P = w["V"].pattern()
+    cuts = shard.row_partition(P.inc_ptr(), world)
+    blk = shard.RowBlock(w["V"], int(cuts[rank]), int(cuts[rank + 1]))
+    S = w["S"]
+    cells = w["mesh"].num_cells()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        S.assemble_into(P, blk.vals, blk.b)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        sustain(step, 0.6)
+        l0 = _capi.kernel_launches()
+        ms = float(np.mean(time_steps(step, args.steps, flush)))
+        launches = _capi.kernel_launches() - l0
+        sustain(step, 0.4)
+    ms_max = shard.max_over_ranks(ms) if dist else ms
+    peak, peak_kind = load_peaks()
+    B = algorithmic_bytes(w)
+    h_vals = torch.empty(blk.nnz, dtype=torch.float64, pin_memory=True)
+    h_b = torch.empty(blk.nrows, dtype=torch.float64, pin_memory=True)
+    h_in = [torch.from_numpy(np.ascontiguousarray(w["x"])).pin_memory()] if w["kind"] == "elasticity" else \
+        [torch.from_numpy(w["fields"]["kappa"]).pin_memory(), torch.from_numpy(w["fields"]["f"]).pin_memory()]
+
+    def e2e_step():
+        if w["kind"] == "elasticity":
+            w["mesh"].set_coordinates(h_in[0].numpy())
+        else:
+            for fobj, hsrc in zip(w["funcs"], h_in):
+                fobj.tensor().copy_(hsrc, non_blocking=True)
+        step()
+        h_vals.copy_(blk.vals, non_blocking=True)
+        h_b.copy_(blk.b, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        e2e_step()
+    e2e_ms = (time.perf_counter() - t0) / 3 * 1e3
+    e2e_ms = shard.max_over_ranks(e2e_ms) if dist else e2e_ms
+    if rank == 0:
+        _, n, deg, desc = WORKLOADS[args.workload]
+        achieved = B / (ms_max * 1e-3) / 1e9
+        line = {
+            "metric": METRIC, "value": round(cells / (ms_max * 1e-3) / 1e6, 3), "unit": "Mcells/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 4),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded jittered unit-cube mesh; no external dataset)",
+            "config": {"workload": args.workload, "description": desc, "cells": cells,
+                       "parallelism": f"row blocks x{world} (one mesh, rows split by incidence count)",
+                       "rank0_rows": blk.nrows, "rank0_nnz": blk.nnz,
+                       "l2": "flushed between steps (256 MiB write)", "parity": PARITY_NOTE},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak * world, "unit": "GB/s",
+                         "frac": round(achieved / (peak * world), 4), "traffic": None,
+                         "peak_source": f"{peak_kind} x{world} GPUs", "algorithmic_bytes": B},
+            "e2e": {"value": round(cells / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mcells/s",
+                    "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": sum(t.numel() * 8 for t in h_in),
+                    "d2h_bytes_per_step": 8 * (blk.nnz + blk.nrows)},
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_profile(args):
     """Only the hot loop of one workload (for ncu captures): warm-up plus
     --steps assembly steps (or matrix-free actions with --profile action),
@@ -649,6 +744,9 @@ def main():
     ap.add_argument("--profile", choices=["step", "action"], default=None,
                     help="run only the hot loop (for ncu), print no JSON")
     ap.add_argument("--mesh-n", type=int, default=None, help="mesh size override (with --profile)")
+    ap.add_argument("--split", choices=["replicas", "rows"], default="replicas",
+                    help="N>1: independent replicas per rank (weak scaling) or one mesh whose node "
+                         "rows are split into per-rank row blocks (strong scaling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -680,6 +778,10 @@ def main():
         if dist:
             dist.barrier()
             dist.destroy_process_group()
+        return
+
+    if args.split == "rows":
+        run_split_rows(args, rank, world, local, dist)
         return
 
     w = setup_workload(args.workload, seed=1000 + rank, device=local)
@@ -745,8 +847,7 @@ def main():
         if w["kind"] == "elasticity":
             mesh.set_coordinates(h_in[0].numpy())  # host -> device coordinate upload
         else:
-            fs = [c for c in w["a"].coefficients()[0]] + [c for c in w["L"].coefficients()[0]]
-            for fobj, hsrc in zip(fs, h_in):
+            for fobj, hsrc in zip(w["funcs"], h_in):
                 fobj.tensor().copy_(hsrc, non_blocking=True)
         S.assemble(A, b)
         h_vals.copy_(A.values_tensor(), non_blocking=True)

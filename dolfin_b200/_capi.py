@@ -18,7 +18,7 @@ ERR_NAMES = {1: "argument", 2: "shape", 3: "index", 4: "mesh", 5: "unsupported",
 
 FORM_DIFFUSION, FORM_LOAD, FORM_ELASTICITY = 1, 2, 3
 FORM_FACET_MASS, FORM_FACET_LOAD, FORM_FUNCTIONAL, FORM_FACET_FUNCTIONAL = 4, 5, 6, 7
-COEFF_NONE, COEFF_CONSTANT, COEFF_P1, COEFF_P1_SCALED, COEFF_COORD = 0, 1, 2, 3, 4
+COEFF_NONE, COEFF_CONSTANT, COEFF_P1, COEFF_P1_SCALED, COEFF_COORD, COEFF_P1_KAPPA = 0, 1, 2, 3, 4, 5
 FP64, FP32_CONTRACT = 0, 1
 
 
@@ -58,6 +58,9 @@ _SIGS = {
     "db2_mesh_write_xml": [P, C.c_char_p],
     "db2_mesh_read_xdmf": [C.c_char_p, PP],
     "db2_pattern_set_row_range": [P, C.c_int64, C.c_int64],
+    "db2_pattern_set_row_block": [P, C.c_int64, C.c_int64],
+    "db2_pattern_row_block_info": [P, P, P],
+    "db2_pattern_row_block_csr_host": [P, P, P],
     "db2_mesh_write_xdmf": [P, C.c_char_p, P, C.c_int, C.c_char_p],
     "db2_vector_write_xml": [C.c_char_p, I64, P],
     "db2_vector_read_xml": [C.c_char_p, C.POINTER(I64), P],

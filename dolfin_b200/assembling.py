@@ -51,6 +51,12 @@ def _parts(form):
     return parts
 
 
+def _whole(P):
+    if P.holds_row_block():
+        raise RuntimeError("the pattern is set to a row block (shard.RowBlock holds its tensors); "
+                           "set_row_range(0, nnodes) restores whole-matrix assembly")
+
+
 def _check_tensor_dims(tensor, rec):
     # AssemblerBase::init_global_tensor, dolfin/fem/AssemblerBase.cpp:182-191
     if tensor.size(0) != rec.V.dim():
@@ -81,13 +87,18 @@ def assemble(form, tensor=None, form_compiler_parameters=None, add_values=False,
             _check_tensor_dims(A, rec)
             if A.pattern.V is not rec.V:
                 raise RuntimeError("*** Error: tensor pattern belongs to another function space")
+        _whole(A.pattern)
         for i, r in enumerate(parts):
             call("db2_assemble_matrix", A.pattern.handle, C.byref(r.c_form()), _coeff_ptr(r), prec,
                  _ptr(A.values_tensor()), int(bool(add_values) or i > 0), _stream())
         return A
+    if cell is not None and cell.pair is not None:
+        raise NotImplementedError("kappa*f*v*dx is assembled with its bilinear form: use "
+                                  "assemble_system / SystemAssembler")
     b = tensor if tensor is not None else Vector(n=rec.V.dim())
     if b.size() != rec.V.dim():
         raise RuntimeError("*** Error: Unable to assemble form. Reason: Dim 0 of tensor does not match form.")
+    _whole(rec.V.pattern(keep_diagonal))
     for i, r in enumerate(parts):
         call("db2_assemble_vector", rec.V.pattern(keep_diagonal).handle, C.byref(r.c_form()),
              _coeff_ptr(r), _ptr(b.tensor()), int(bool(add_values) or i > 0), _stream())
@@ -161,6 +172,9 @@ class SystemAssembler:
                                  (0.0, 0.0, 0.0))
         if self.ra.V is not self.rL.V:
             raise RuntimeError("a and L must share the function space")
+        if self.rL.pair is not None:
+            # kappa*f*v*dx: kappa is the bilinear form's P1 coefficient
+            self.rL = self.rL.with_kappa(self.ra.function)
         self.bcs = [] if bcs is None else (bcs if isinstance(bcs, (list, tuple)) else [bcs])
         self.prec = _PREC[precision]
         self.keep_diagonal = False
@@ -175,30 +189,36 @@ class SystemAssembler:
             b = Vector(n=V.dim())
         if A is None:
             return self._vector_only(b)
+        _whole(A.pattern)
+        self.assemble_into(A.pattern, A.values_tensor(), b.tensor())
+        return A, b
+
+    def assemble_into(self, P, vt, bt):
+        """Assemble A and b into the device tensors vt (CSR values of pattern
+        P, or its row block) and bt."""
         if self.bcs:
-            flags, vals = _bc_arrays(V, self.bcs)
-            call("db2_assemble_system_bc", A.pattern.handle, C.byref(self.ra.c_form()),
+            flags, vals = _bc_arrays(self.ra.V, self.bcs)
+            call("db2_assemble_system_bc", P.handle, C.byref(self.ra.c_form()),
                  _coeff_ptr(self.ra), C.byref(self.rL.c_form()), _coeff_ptr(self.rL), _ptr(flags),
-                 _ptr(vals), self.prec, _ptr(A.values_tensor()), _ptr(b.tensor()), _stream())
+                 _ptr(vals), self.prec, _ptr(vt), _ptr(bt), _stream())
             if self.ra_ds is not None or self.rL_ds is not None:
                 # exterior-facet terms with the same Dirichlet treatment
                 fa = C.byref(self.ra_ds.c_form()) if self.ra_ds is not None else None
                 fl = C.byref(self.rL_ds.c_form()) if self.rL_ds is not None else None
-                call("db2_assemble_facets_bc", A.pattern.handle, fa,
+                call("db2_assemble_facets_bc", P.handle, fa,
                      _coeff_ptr(self.ra_ds) if self.ra_ds is not None else None, fl,
                      _coeff_ptr(self.rL_ds) if self.rL_ds is not None else None, _ptr(flags),
-                     _ptr(vals), _ptr(A.values_tensor()), _ptr(b.tensor()), _stream())
+                     _ptr(vals), _ptr(vt), _ptr(bt), _stream())
         else:
-            call("db2_assemble_system", A.pattern.handle, C.byref(self.ra.c_form()),
+            call("db2_assemble_system", P.handle, C.byref(self.ra.c_form()),
                  _coeff_ptr(self.ra), C.byref(self.rL.c_form()), _coeff_ptr(self.rL), self.prec,
-                 _ptr(A.values_tensor()), _ptr(b.tensor()), _stream())
+                 _ptr(vt), _ptr(bt), _stream())
             if self.ra_ds is not None:
-                call("db2_assemble_matrix", A.pattern.handle, C.byref(self.ra_ds.c_form()),
-                     _coeff_ptr(self.ra_ds), self.prec, _ptr(A.values_tensor()), 1, _stream())
+                call("db2_assemble_matrix", P.handle, C.byref(self.ra_ds.c_form()),
+                     _coeff_ptr(self.ra_ds), self.prec, _ptr(vt), 1, _stream())
             if self.rL_ds is not None:
-                call("db2_assemble_vector", A.pattern.handle, C.byref(self.rL_ds.c_form()),
-                     _coeff_ptr(self.rL_ds), _ptr(b.tensor()), 1, _stream())
-        return A, b
+                call("db2_assemble_vector", P.handle, C.byref(self.rL_ds.c_form()),
+                     _coeff_ptr(self.rL_ds), _ptr(bt), 1, _stream())
 
     def _vector_only(self, b):
         P = self.rL.V.pattern(False)

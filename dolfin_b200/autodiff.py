@@ -5,7 +5,8 @@ gA (CSR-shaped, over the values of A = assemble(kappa*grad(u).grad(v)*dx))
 and optionally gb (over b = assemble(kappa*f*v*dx)), it returns
 dL/dkappa = sum gA * dA/dkappa + sum gb * db/dkappa -- the assembly of the
 derivative form derivative(a, kappa) contracted with gA.  ``AssembleDiffusion``
-wraps forward assembly and this adjoint in a torch.autograd.Function.
+wraps forward system assembly (A and b) and this adjoint in a
+torch.autograd.Function.
 """
 from __future__ import annotations
 
@@ -36,7 +37,7 @@ def vjp_kappa(V, kappa, gA, f=None, gb=None, precision="fp64", scale=1.0, noallo
     a = _capi.make_form(_capi.FORM_DIFFUSION, _capi.COEFF_P1_SCALED, (scale,))
     L = None
     if f is not None and gb is not None:
-        L = _capi.make_form(_capi.FORM_LOAD, _capi.COEFF_P1_SCALED, (1.0,))
+        L = _capi.make_form(_capi.FORM_LOAD, _capi.COEFF_P1_KAPPA, (1.0,))
         f = f.contiguous().to(torch.float64)
         gb = gb.contiguous().to(torch.float64)
     dk = torch.empty(nv, dtype=torch.float64, device=kappa.device)
@@ -46,29 +47,45 @@ def vjp_kappa(V, kappa, gA, f=None, gb=None, precision="fp64", scale=1.0, noallo
 
 
 class AssembleDiffusion(torch.autograd.Function):
-    """vals = assemble(kappa*inner(grad(u), grad(v))*dx).values on V, differentiable in kappa."""
+    """(A values, b) = assemble_system(kappa*inner(grad(u), grad(v))*dx, L) on
+    V, differentiable in the P1 field kappa:
+
+        L = kappa*f*v*dx   (weighted=True: b depends on kappa), or
+        L = f*v*dx         (weighted=False: b does not),
+
+    f a P1 vertex field (a tensor).  Backward runs the engine's adjoint:
+    dL/dkappa = sum gA dA/dkappa + sum gb db/dkappa for the upstream
+    gradients gA (over the CSR values) and gb (over b).
+
+        vals, b = AssembleDiffusion.apply(kappa, V, f, True, "fp64")
+    """
 
     @staticmethod
-    def forward(ctx, kappa, V, precision="fp64"):
-        from .assembling import assemble
+    def forward(ctx, kappa, V, f, weighted=True, precision="fp64"):
+        from .assembling import SystemAssembler
         from .function import Function
         from .cpp import FunctionSpace
         from .ufl import TestFunction, TrialFunction, dx, grad, inner
-        W = V._p1_space if hasattr(V, "_p1_space") else None
+        W = getattr(V, "_p1_space", None)
         if W is None:
             W = FunctionSpace(V.mesh(), "Lagrange", 1)
             V._p1_space = W
-        k = Function.__new__(Function)
-        Function.__init__(k, W)
-        k._x = kappa.detach().contiguous().to(torch.float64)
+        kt = kappa.detach().contiguous().to(torch.float64)
+        ft = f.detach().contiguous().to(torch.float64)
+        k, fn = Function(W, kt), Function(W, ft)  # device tensors, not copied
         u, v = TrialFunction(V), TestFunction(V)
-        A = assemble(k * inner(grad(u), grad(v)) * dx, precision=precision)
-        ctx.save_for_backward(kappa)
-        ctx.V, ctx.precision = V, precision
-        return A.values_tensor()
+        L = (k * fn * v * dx) if weighted else (fn * v * dx)
+        A, b = SystemAssembler(k * inner(grad(u), grad(v)) * dx, L, precision=precision).assemble()
+        ctx.save_for_backward(kt, ft)
+        ctx.V, ctx.precision, ctx.weighted = V, precision, weighted
+        return A.values_tensor(), b.tensor()
 
     @staticmethod
-    def backward(ctx, gvals):
-        (kappa,) = ctx.saved_tensors
-        dk = vjp_kappa(ctx.V, kappa.detach(), gvals.contiguous(), precision=ctx.precision)
-        return dk, None, None
+    def backward(ctx, gvals, gb):
+        kt, ft = ctx.saved_tensors
+        if gvals is None:
+            gvals = torch.zeros(ctx.V.pattern().nnz(), dtype=torch.float64, device=kt.device)
+        use_b = ctx.weighted and gb is not None
+        dk = vjp_kappa(ctx.V, kt, gvals.contiguous(), f=ft if use_b else None,
+                       gb=gb.contiguous() if use_b else None, precision=ctx.precision)
+        return dk, None, None, None, None

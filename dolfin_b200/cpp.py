@@ -307,6 +307,15 @@ class SparsityPattern(_Handle):
         return dict(node_rowptr=node_rowptr, node_cols=node_cols, inc_ptr=inc_ptr, inc=inc,
                     pos=pos.reshape(ninc, kp), tiles=tiles, kp=kp)
 
+    def inc_ptr(self):
+        """Node -> incidence offsets alone (the work weights of the rows)."""
+        nn, ninc, kp, nt = C.c_int64(), C.c_int64(), C.c_int(), C.c_int64()
+        call("db2_pattern_plan_info", self._h, C.byref(nn), C.byref(ninc), C.byref(kp), C.byref(nt),
+             None, None)
+        out = np.empty(nn.value + 1, np.uint32)
+        call("db2_pattern_plan_copy", self._h, None, None, _ptr(out), None, None, None)
+        return out
+
     def retile(self, tile_threads, seg_cap_bytes):
         """Launch shape of the assembly kernel (see db2_pattern_retile)."""
         call("db2_pattern_retile", self._h, int(tile_threads), int(seg_cap_bytes))
@@ -315,6 +324,30 @@ class SparsityPattern(_Handle):
         """Assemble only the rows of nodes [node_begin, node_end) (a rank's
         share of a row-partitioned assembly; see db2_pattern_set_row_range)."""
         call("db2_pattern_set_row_range", self._h, int(node_begin), int(node_end))
+        self._block = False
+
+    def set_row_block(self, node_begin, node_end):
+        """As set_row_range, with the tensors holding the row block alone
+        (a rank's own rows; see db2_pattern_set_row_block)."""
+        call("db2_pattern_set_row_block", self._h, int(node_begin), int(node_end))
+        self._block = True
+
+    def holds_row_block(self):
+        return getattr(self, "_block", False)
+
+    def row_block_info(self):
+        """(rows, nonzeros) of the current row block."""
+        nr, nz = C.c_int64(), C.c_int64()
+        call("db2_pattern_row_block_info", self._h, C.byref(nr), C.byref(nz))
+        return int(nr.value), int(nz.value)
+
+    def row_block_csr_host(self):
+        """The row block's CSR: row pointers from 0 and global columns."""
+        nr, nz = self.row_block_info()
+        rp = np.empty(nr + 1, np.int32)
+        cols = np.empty(nz, np.int32)
+        call("db2_pattern_row_block_csr_host", self._h, _ptr(rp), _ptr(cols))
+        return rp, cols
 
 
 def _wrap_device(ptr, n, dtype, owner):

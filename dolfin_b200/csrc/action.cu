@@ -445,11 +445,12 @@ void launch_vjp(const Pattern& P, const FormArgs& a, const FormArgs& L, int prec
   p.kappa = a.w;
   // L = kappa * f * v * dx contributes when its coefficient is P1_SCALED
   // (the kappa-weighted load); any other load does not depend on kappa.
-  const bool loadk = gb && L.f.kind == DB2_FORM_LOAD && L.f.coeff == DB2_COEFF_P1_SCALED;
+  const bool loadk = gb && L.f.kind == DB2_FORM_LOAD &&
+                     (L.f.coeff == DB2_COEFF_P1_SCALED || L.f.coeff == DB2_COEFF_P1_KAPPA);
   if (loadk) {
     if (!L.w) fail(DB2_ERR_ARGUMENT, "kappa-weighted load needs its P1 field f");
     p.f = L.w;
-    p.fc[0] = 1.0;
+    p.fc[0] = L.f.coeff == DB2_COEFF_P1_KAPPA ? L.f.constant[0] : 1.0;
   }
   const int D = P.V->mesh->tdim, deg = P.V->degree;
   const int64_t nc = P.V->mesh->nc, nv = P.V->mesh->nv;

@@ -33,7 +33,9 @@ namespace db2 {
 namespace dev {
 
 enum { FORM_DIFF = 0, FORM_ELAS = 1 };
-enum { LOAD_NONE = 0, LOAD_CONST = 1, LOAD_P1 = 2 };
+// loads: none, constant f, P1 f, and kappa*f with the bilinear form's P1
+// kappa (the kappa-weighted load whose derivative the adjoint also takes)
+enum { LOAD_NONE = 0, LOAD_CONST = 1, LOAD_P1 = 2, LOAD_KP1 = 3 };
 #ifndef DB2_TILE_MAX_THREADS
 #define DB2_TILE_MAX_THREADS 256
 #endif
@@ -300,6 +302,12 @@ struct AsmParams {
   double* b;
   int64_t nnz_node;
   int64_t nnodes;
+  // output layout: value (c, k) of the CSR at vals[c * vstride + k - vbase],
+  // b entry (c, node) at b[c * bstride + node - bbase] -- the full arrays
+  // (vstride = bs nnz_node, bstride = nnodes, bases 0), or a rank's row
+  // block of nodes [n0, n1) held alone (vstride = bs (rowptr[n1] -
+  // rowptr[n0]), vbase = bs rowptr[n0], bstride = n1 - n0, bbase = n0)
+  int64_t vstride, vbase, bstride, bbase;
   int64_t nverts;
   int add_values;
   const uint8_t* bc_flags;   // dof-level Dirichlet flags or null
@@ -623,7 +631,8 @@ __device__ __forceinline__ void element_row(const AsmParams& p, const Geometry<D
 
 template <int D, int P, int LOADM>
 __device__ __forceinline__ double load_row(const AsmParams& p, const Geometry<D>& G, bool vertex,
-                                           int c, const double (&fv)[D + 1]) {
+                                           int c, const double (&fv)[D + 1],
+                                           const double (&kap)[D + 1]) {
   using R = Rows<D, P, double>;
   if constexpr (LOADM == LOAD_CONST) {
     double r;
@@ -634,6 +643,19 @@ __device__ __forceinline__ double load_row(const AsmParams& p, const Geometry<D>
     double r;
     if constexpr (P == 2) r = vertex ? R::v_fp1(fv) : R::e_fp1(fv);
     else r = R::v_fp1(fv);
+    return G.vol * r * p.fc[0];
+  } else if constexpr (LOADM == LOAD_KP1) {
+    // int kappa f phi_i = sum_m kappa_m int lambda_m f phi_i (kappa P1)
+    double o[D + 1];
+    if constexpr (P == 2) {
+      if (vertex) R::v_kfp1(fv, o);
+      else R::e_kfp1(fv, o);
+    } else {
+      R::v_kfp1(fv, o);
+    }
+    double r = kap[0] * o[0];
+#pragma unroll
+    for (int m = 1; m <= D; ++m) r = fma(kap[m], o[m], r);
     return G.vol * r * p.fc[0];
   } else {
     return 0.0;
@@ -648,7 +670,7 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
                                          double* bpart, int32_t r0, int u) {
   using E = El<D, P>;
   constexpr int BS = FORM == FORM_ELAS ? D : 1;
-  constexpr bool FP1 = LOADM == LOAD_P1;
+  constexpr bool FP1 = LOADM == LOAD_P1 || LOADM == LOAD_KP1;
   constexpr bool vertex = NFIX == 1;
   const bool bc = p.bc_flags != nullptr;
   const uint32_t node = t.n0 + u / BS;
@@ -719,14 +741,14 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
     CT out[E::K];
     element_row<D, P, FORM, KP1, CT>(p, G, vertex, t.comp, e, kap, out);
     if constexpr (LOADM != LOAD_NONE) {
-      if (e == 0) bsum += load_row<D, P, LOADM>(p, G, vertex, t.comp, fv);
+      if (e == 0) bsum += load_row<D, P, LOADM>(p, G, vertex, t.comp, fv, kap);
     }
     if (bc) {
       if (row_bc) {
 #pragma unroll
         for (int j = 0; j < E::K; ++j) out[j] = CT((e == t.comp && j == jstar) ? 1 : 0);
         if constexpr (LOADM != LOAD_NONE) {
-          if (e == 0) bsum = bsum - load_row<D, P, LOADM>(p, G, vertex, t.comp, fv) + row_g;
+          if (e == 0) bsum = bsum - load_row<D, P, LOADM>(p, G, vertex, t.comp, fv, kap) + row_g;
         }
       } else {
 #pragma unroll
@@ -799,11 +821,11 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
       double s = 0.0;
 #pragma unroll
       for (int e = 0; e < BS; ++e) s += bpart[i * BS + e];
-      double* bp = p.b + int64_t(t.comp) * p.nnodes + t.n0 + i;
+      double* bp = p.b + int64_t(t.comp) * p.bstride + (t.n0 - p.bbase) + i;
       *bp = p.add_values ? *bp + s : s;
     }
   }
-  double* dst = p.vals + int64_t(t.comp) * BS * p.nnz_node + int64_t(BS) * r0;
+  double* dst = p.vals + int64_t(t.comp) * p.vstride + int64_t(BS) * r0 - p.vbase;
   if (p.add_values) {
     for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] += acc[i];
   } else {

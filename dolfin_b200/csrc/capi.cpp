@@ -350,6 +350,41 @@ int db2_pattern_set_row_range(db2_pattern P, int64_t node_begin, int64_t node_en
   });
 }
 
+int db2_pattern_set_row_block(db2_pattern P, int64_t node_begin, int64_t node_end) {
+  return guard([&] {
+    need(P, "pattern");
+    db2::set_row_range(*P->P, node_begin, node_end, true);
+  });
+}
+
+int db2_pattern_row_block_info(db2_pattern P, int64_t* nrows, int64_t* nnz) {
+  return guard([&] {
+    need(P, "pattern");
+    db2::row_block_size(*P->P, nrows, nnz);
+  });
+}
+
+int db2_pattern_row_block_csr_host(db2_pattern P, int32_t* rowptr, int32_t* cols) {
+  return guard([&] {
+    need(P, "pattern");
+    const db2::Pattern& Q = *P->P;
+    if (Q.V->reordered()) db2::fail(DB2_ERR_UNSUPPORTED, "row blocks are provided for the natural numbering");
+    const int64_t nn = Q.V->nnodes, n0 = Q.row_begin, n1 = Q.row_end < 0 ? nn : Q.row_end;
+    const int bs = Q.bs;
+    int64_t at = 0, r = 0;
+    for (int c = 0; c < bs; ++c)
+      for (int64_t i = n0; i < n1; ++i, ++r) {
+        const int32_t a = Q.node_rowptr[i], L = Q.node_rowptr[i + 1] - a;
+        if (rowptr) rowptr[r] = int32_t(at);
+        if (cols)
+          for (int e = 0; e < bs; ++e)
+            for (int32_t t = 0; t < L; ++t) cols[at + int64_t(e) * L + t] = int32_t(e * nn + Q.node_cols[a + t]);
+        at += int64_t(bs) * L;
+      }
+    if (rowptr) rowptr[r] = int32_t(at);
+  });
+}
+
 int db2_pattern_facet_plan_info(db2_pattern P, int64_t* nbnodes, int64_t* nincidences, int* kf) {
   return guard([&] {
     need(P, "pattern");
@@ -565,6 +600,8 @@ int db2_vjp_kappa(db2_pattern P, const db2_form* a, const double* kappa, const d
       fl.f.coeff = DB2_COEFF_NONE;
     }
     db2::Pattern& Pt = *P->P;
+    if (Pt.block_storage)
+      db2::fail(DB2_ERR_UNSUPPORTED, "the adjoint takes whole-CSR gradients (no row-block storage)");
     if (Pt.V->reordered()) {
       // upstream gradients into the natural numbering
       db2::ReorderedCSR& R = db2::reordered_on_device(Pt);

@@ -45,6 +45,8 @@ struct FacetParams {
   // boundary nodes handled by this launch: bnode[bn0 .. bn0 + nbnodes), the
   // ones inside the pattern's row range
   int64_t bn0, nbnodes;
+  // output layout of the pattern (full arrays or a rank's row block)
+  int64_t vbase, bstride, bbase;
   int bs;
 };
 
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(256) k_facet_vector(const FacetParams p) {
   for (int c = 0; c < p.bs; ++c) {
     const int64_t dof = int64_t(c) * p.nnodes + node;
     if (p.bc_flags && __ldg(p.bc_flags + dof)) continue;
-    p.b[dof] += (p.bs == 1 ? p.scale : p.t[c]) * acc;
+    p.b[int64_t(c) * p.bstride + node - p.bbase] += (p.bs == 1 ? p.scale : p.t[c]) * acc;
   }
 }
 
@@ -98,7 +100,7 @@ __global__ void __launch_bounds__(256) k_facet_matrix(const FacetParams p) {
   if (p.bc_flags && __ldg(p.bc_flags + node)) return;
   const bool vertex = P == 1 || node < p.nverts;
   const int32_t ra = __ldg(p.rowptr + node);
-  double* row = p.vals + ra;
+  double* row = p.vals + ra - p.vbase;
   double bsub = 0.0;
   const uint32_t s1 = __ldg(p.binc_ptr + t + 1);
   for (uint32_t s = __ldg(p.binc_ptr + t); s < s1; ++s) {
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(256) k_facet_matrix(const FacetParams p) {
       row[slot] += v;
     }
   }
-  if (p.bc_flags && bsub != 0.0) p.b[node] -= bsub;
+  if (p.bc_flags && bsub != 0.0) p.b[node - p.bbase] -= bsub;
 }
 
 // ---- functionals ------------------------------------------------------------
@@ -263,6 +265,10 @@ dev::FacetParams facet_params(Pattern& P) {
   p.bn0 = int64_t(lo - F.bnode.begin());
   p.nbnodes = int64_t(hi - lo);
   p.bs = P.V->vsize;
+  const OutputLayout o = output_layout(P);
+  p.vbase = o.vbase;
+  p.bstride = o.bstride;
+  p.bbase = o.bbase;
   return p;
 }
 
@@ -272,13 +278,15 @@ dev::FacetParams facet_params(Pattern& P) {
 void zero_range_values(const Pattern& P, double* vals, cudaStream_t s) {
   const int64_t r0 = P.row_begin, r1 = P.row_end < 0 ? P.V->nnodes : P.row_end;
   const int64_t v0 = P.node_rowptr[r0], v1 = P.node_rowptr[r1];
-  if (v1 > v0) cudaMemsetAsync(vals + v0, 0, size_t(v1 - v0) * sizeof(double), s);
+  const OutputLayout o = output_layout(P);
+  if (v1 > v0) cudaMemsetAsync(vals + v0 - o.vbase, 0, size_t(v1 - v0) * sizeof(double), s);
 }
 void zero_range_dofs(const Pattern& P, double* b, cudaStream_t s) {
   const int64_t r0 = P.row_begin, r1 = P.row_end < 0 ? P.V->nnodes : P.row_end;
   if (r1 <= r0) return;
+  const OutputLayout o = output_layout(P);
   for (int c = 0; c < P.V->vsize; ++c)
-    cudaMemsetAsync(b + int64_t(c) * P.V->nnodes + r0, 0, size_t(r1 - r0) * sizeof(double), s);
+    cudaMemsetAsync(b + int64_t(c) * o.bstride + r0 - o.bbase, 0, size_t(r1 - r0) * sizeof(double), s);
 }
 
 template <typename K>

@@ -555,7 +555,7 @@ void retile(Pattern& P, int tile_threads, int seg_cap_bytes) {
 // node_end) completely from the cells around them (their incidence lists),
 // with no exchange -- the row-owner analogue of DOLFIN's owned-row ranges
 // (SparsityPattern.cpp:200-255).  Only the tile kernel is restricted.
-void set_row_range(Pattern& P, int64_t node_begin, int64_t node_end) {
+void set_row_range(Pattern& P, int64_t node_begin, int64_t node_end, bool block_storage) {
   const int64_t nn = P.V->nnodes;
   if (node_begin < 0 || node_end < node_begin || node_end > nn)
     fail(DB2_ERR_ARGUMENT, "row range [%lld, %lld) outside [0, %lld)", (long long)node_begin,
@@ -564,8 +564,22 @@ void set_row_range(Pattern& P, int64_t node_begin, int64_t node_end) {
     fail(DB2_ERR_UNSUPPORTED, "row ranges are provided for the natural numbering");
   P.row_begin = node_begin;
   P.row_end = node_end == nn ? -1 : node_end;
+  P.block_storage = block_storage;
   build_tiles(P, P.tile_threads, P.seg_cap_bytes / 8);
   if (P.on_device) P.d_tiles.upload(P.tiles.data(), P.tiles.size() * sizeof(Tile));
+}
+
+OutputLayout output_layout(const Pattern& P) {
+  const int64_t bs = P.bs;
+  if (!P.block_storage) return OutputLayout{bs * P.nnz_node, 0, P.V->nnodes, 0};
+  const int64_t n0 = P.row_begin, n1 = P.row_end < 0 ? P.V->nnodes : P.row_end;
+  return OutputLayout{bs * (P.node_rowptr[n1] - P.node_rowptr[n0]), bs * P.node_rowptr[n0], n1 - n0, n0};
+}
+
+void row_block_size(const Pattern& P, int64_t* nrows, int64_t* nnz) {
+  const int64_t n0 = P.row_begin, n1 = P.row_end < 0 ? P.V->nnodes : P.row_end;
+  if (nrows) *nrows = (n1 - n0) * P.bs;
+  if (nnz) *nnz = int64_t(P.bs) * P.bs * (P.node_rowptr[n1] - P.node_rowptr[n0]);
 }
 
 std::shared_ptr<Pattern> make_pattern(std::shared_ptr<Space> V, bool keep_diagonal,

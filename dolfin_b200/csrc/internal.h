@@ -138,6 +138,10 @@ struct Pattern {
   // node rows the tile kernel assembles: [row_begin, row_end) (a rank's share
   // of a row-partitioned assembly); row_end < 0 = all rows
   int64_t row_begin = 0, row_end = -1;
+  // the caller's value and vector arrays hold the row block alone (a rank's
+  // CSR rows of nodes [row_begin, row_end), every component, in global row
+  // order; b likewise) instead of the whole CSR / vector
+  bool block_storage = false;
 
   int seg_cap = 0;                   // doubles of shared memory of the largest tile
   // Device incidence records (rs = 8 or 16 bytes, one vector load each):
@@ -202,7 +206,14 @@ void retile(Pattern& P, int tile_threads, int seg_cap_bytes);
 // Tiles of a pattern for a launch shape (pure; does not modify P).
 std::vector<Tile> cut_tiles(const Pattern& P, int tile_threads, int seg_cap_doubles, int* max_seg,
                             int64_t node_begin = 0, int64_t node_end = -1);
-void set_row_range(Pattern& P, int64_t node_begin, int64_t node_end);
+void set_row_range(Pattern& P, int64_t node_begin, int64_t node_end, bool block_storage = false);
+// Where the kernels put CSR value (c, k) and b entry (c, node): see AsmParams.
+struct OutputLayout {
+  int64_t vstride, vbase, bstride, bbase;
+};
+OutputLayout output_layout(const Pattern& P);
+// Size of a pattern's row block (the whole pattern without a range).
+void row_block_size(const Pattern& P, int64_t* nrows, int64_t* nnz);
 
 // Launchers (kernels.cu).  All return after enqueueing on `stream`.
 struct FormArgs {

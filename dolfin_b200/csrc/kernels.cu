@@ -10,11 +10,12 @@ namespace dev {
 // Vector-only assembly (Assembler::assemble for a rank-1 form): one thread
 // per dof (component c, node i) gathering its incident cells in cell order.
 template <int D, int P, int LOADM>
-__global__ void __launch_bounds__(256) k_assemble_vector(const AsmParams p, int bs) {
+__global__ void __launch_bounds__(256) k_assemble_vector(const AsmParams p, int bs, int64_t n0,
+                                                         int64_t nrange) {
   const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (r >= p.nnodes * bs) return;
-  const int c = int(r / p.nnodes);
-  const int64_t node = r - int64_t(c) * p.nnodes;
+  if (r >= nrange * bs) return;
+  const int c = int(r / nrange);
+  const int64_t node = n0 + (r - int64_t(c) * nrange);
   double bsum = 0.0;
   const uint32_t i0 = __ldg(p.inc_ptr + node);
   const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - i0;
@@ -26,9 +27,9 @@ __global__ void __launch_bounds__(256) k_assemble_vector(const AsmParams p, int 
     record_cell<D, P, LOADM == LOAD_P1>(p, F, r, i0 + m, x, kap, fv);
     Geometry<D> G;
     geometry(x, G);
-    bsum += load_row<D, P, LOADM>(p, G, F.nfix == 1, c, fv);
+    bsum += load_row<D, P, LOADM>(p, G, F.nfix == 1, c, fv, kap);
   }
-  double* bp = p.b + r;
+  double* bp = p.b + int64_t(c) * p.bstride + node - p.bbase;
   *bp = p.add_values ? *bp + bsum : bsum;
 }
 
@@ -83,6 +84,11 @@ dev::AsmParams make_params(const Pattern& P) {
   p.fc[0] = p.fc[1] = p.fc[2] = 0.0;
   p.nnz_node = P.nnz_node;
   p.nnodes = P.V->nnodes;
+  const OutputLayout o = output_layout(P);
+  p.vstride = o.vstride;
+  p.vbase = o.vbase;
+  p.bstride = o.bstride;
+  p.bbase = o.bbase;
   return p;
 }
 
@@ -118,6 +124,12 @@ static int load_mode(const FormArgs* L, int bs, dev::AsmParams& p) {
       p.f = L->w;
       p.fc[0] = L->f.coeff == DB2_COEFF_P1 ? 1.0 : L->f.constant[0];
       return dev::LOAD_P1;
+    case DB2_COEFF_P1_KAPPA:
+      if (bs != 1) fail(DB2_ERR_UNSUPPORTED, "kappa-weighted load on a vector space");
+      if (!L->w) fail(DB2_ERR_ARGUMENT, "kappa-weighted load: no field f was given");
+      p.f = L->w;
+      p.fc[0] = L->f.constant[0];
+      return dev::LOAD_KP1;
     default: fail(DB2_ERR_ARGUMENT, "unknown coefficient kind %d", L->f.coeff);
   }
 }
@@ -134,18 +146,25 @@ void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int
   p.bc_flags = bc_flags;
   p.bc_vals = bc_vals;
   const int loadm = load_mode(L, P.bs, p);
+  if (loadm == dev::LOAD_KP1 && !(a && a->f.kind == DB2_FORM_DIFFUSION &&
+                                  (a->f.coeff == DB2_COEFF_P1 || a->f.coeff == DB2_COEFF_P1_SCALED)))
+    fail(DB2_ERR_UNSUPPORTED, "a kappa-weighted load (DB2_COEFF_P1_KAPPA) is assembled together with "
+         "kappa*grad(u).grad(v)*dx with a P1 kappa (db2_assemble_system / _system_bc)");
   if (!a) {
     pack_vertex_records(P, nullptr, loadm == dev::LOAD_P1 ? p.f : nullptr, stream);
     // rank-1 form only
     if (loadm == dev::LOAD_NONE) fail(DB2_ERR_ARGUMENT, "nothing to assemble");
-    const int64_t n = V.nnodes * P.bs;
+    // the node rows of the pattern's row range (all of them by default)
+    const int64_t n0 = P.row_begin, nr = (P.row_end < 0 ? V.nnodes : P.row_end) - n0;
+    const int64_t n = nr * P.bs;
+    if (n == 0) return;
     const int threads = 256;
     const unsigned blocks = unsigned((n + threads - 1) / threads);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 #define DB2_VEC(D_, P_)                                                                       \
   if (D == D_ && V.degree == P_) {                                                            \
-    if (loadm == dev::LOAD_CONST) dev::k_assemble_vector<D_, P_, dev::LOAD_CONST><<<blocks, threads, 0, s>>>(p, P.bs); \
-    else dev::k_assemble_vector<D_, P_, dev::LOAD_P1><<<blocks, threads, 0, s>>>(p, P.bs);    \
+    if (loadm == dev::LOAD_CONST) dev::k_assemble_vector<D_, P_, dev::LOAD_CONST><<<blocks, threads, 0, s>>>(p, P.bs, n0, nr); \
+    else dev::k_assemble_vector<D_, P_, dev::LOAD_P1><<<blocks, threads, 0, s>>>(p, P.bs, n0, nr);    \
     count_launch();                                                                           \
     check_cuda("assemble_vector launch");                                                     \
     return;                                                                                   \
@@ -168,7 +187,8 @@ void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int
   if (a->f.kind == DB2_FORM_DIFFUSION) {
     if (P.bs != 1) fail(DB2_ERR_UNSUPPORTED, "diffusion form on a vector space");
     const bool kp1 = matrix_coeff(*a, p);
-    pack_vertex_records(P, kp1 ? p.kappa : nullptr, loadm == dev::LOAD_P1 ? p.f : nullptr, stream);
+    pack_vertex_records(P, kp1 ? p.kappa : nullptr,
+                        (loadm == dev::LOAD_P1 || loadm == dev::LOAD_KP1) ? p.f : nullptr, stream);
     ok = D == 3 ? dev::dispatch_tet_diff(V.degree, p, cfg, kp1, loadm, fp32)
                 : dev::dispatch_tri_diff(V.degree, p, cfg, kp1, loadm, fp32);
   } else if (a->f.kind == DB2_FORM_ELASTICITY) {

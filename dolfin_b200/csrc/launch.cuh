@@ -121,6 +121,7 @@ bool dispatch(const AsmParams& p, const LaunchCfg& cfg, bool kp1, int loadm, boo
       if (loadm == LOAD_NONE) DB2_RUN(true, LOAD_NONE);
       if (loadm == LOAD_CONST) DB2_RUN(true, LOAD_CONST);
       if (loadm == LOAD_P1) DB2_RUN(true, LOAD_P1);
+      if (loadm == LOAD_KP1) DB2_RUN(true, LOAD_KP1);
     } else {
       if (loadm == LOAD_NONE) DB2_RUN(false, LOAD_NONE);
       if (loadm == LOAD_CONST) DB2_RUN(false, LOAD_CONST);

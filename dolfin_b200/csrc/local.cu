@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(256) k_local_cell(const AsmParams p,
       for (int j = 0; j < K; ++j) row[e * K + int((mc >> (4 * j)) & 15u)] = o[j];
     }
   } else {
-    out[size_t(idx) * n + c * K + li] = load_row<D, P, LOADM>(p, G, vertex, c, fv);
+    out[size_t(idx) * n + c * K + li] = load_row<D, P, LOADM>(p, G, vertex, c, fv, kap);
   }
 }
 

@@ -92,6 +92,8 @@ extern "C" int db2_vjp_kappa_noalloc(db2_pattern Ph, const db2_form* a, const do
       fail(DB2_ERR_UNSUPPORTED,
            "db2_vjp_kappa_noalloc does not take patterns on reordered spaces (their gradients "
            "need library scratch); use db2_vjp_kappa");
+    if (P->block_storage)
+      fail(DB2_ERR_UNSUPPORTED, "the adjoint takes whole-CSR gradients (no row-block storage)");
     if (!P->on_device)
       fail(DB2_ERR_ARGUMENT,
            "pattern is not resident on the device yet; assemble with it (or call "

@@ -38,6 +38,57 @@ def row_partition(inc_ptr, nranks):
     return np.concatenate([[0], cuts, [len(inc_ptr) - 1]]).astype(np.int64)
 
 
+def row_block_dofs(nnodes, bs, node_begin, node_end):
+    """Global dof numbers of a row block (natural numbering), in the order
+    the block stores them: component-major, nodes ascending."""
+    nodes = np.arange(node_begin, node_end, dtype=np.int64)
+    return np.concatenate([c * nnodes + nodes for c in range(bs)])
+
+
+class RowBlock:
+    """One rank's share of a single-mesh assembly: the CSR rows and b entries
+    of nodes [node_begin, node_end) (every component), assembled from the
+    cells around them and held alone -- the rank allocates its block, not
+    the whole matrix.  The row-owner counterpart of DOLFIN's distributed
+    SparsityPattern (dolfin/la/SparsityPattern.cpp:200-255): ranks exchange
+    nothing, since no rank produces entries of rows it does not own.
+
+        blk = RowBlock(V, n0, n1)
+        blk.assemble_system(a, L)       # blk.vals, blk.b (device, local)
+    """
+
+    def __init__(self, V, node_begin, node_end, keep_diagonal=False):
+        import torch
+        self.V = V
+        self.pattern = V.pattern(keep_diagonal)
+        self.node_begin, self.node_end = int(node_begin), int(node_end)
+        self.pattern.set_row_block(self.node_begin, self.node_end)
+        self.nrows, self.nnz = self.pattern.row_block_info()
+        self.vals = torch.empty(self.nnz, dtype=torch.float64, device="cuda")
+        self.b = torch.empty(self.nrows, dtype=torch.float64, device="cuda")
+
+    def dofs(self):
+        """Global dofs of the block's rows (its b entries), in block order."""
+        nn = self.V.dim() // self.V.value_size()
+        return row_block_dofs(nn, self.V.value_size(), self.node_begin, self.node_end)
+
+    def csr_host(self):
+        return self.pattern.row_block_csr_host()
+
+    def assemble_system(self, a, L, bcs=None, precision="fp64"):
+        """SystemAssembler(a, L, bcs) restricted to the block's rows."""
+        from .assembling import SystemAssembler
+        S = SystemAssembler(a, L, bcs, precision)
+        if S.ra.V is not self.V:
+            raise RuntimeError("the forms live on another function space")
+        S.assemble_into(self.pattern, self.vals, self.b)
+        return self.vals, self.b
+
+    def release(self):
+        """Back to whole-pattern assembly (all rows, whole tensors)."""
+        self.pattern.set_row_range(0, self.V.dim() // self.V.value_size())
+
+
 def max_over_ranks(value, group=None):
     """Max of a per-rank scalar (e.g. device time in ms) over the process group."""
     import torch

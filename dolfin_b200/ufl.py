@@ -357,9 +357,23 @@ class Form:
 class Recognised:
     """Identified form: kind, coefficient, constants, space."""
 
-    def __init__(self, kind, V, coeff, function=None, constant=(0.0, 0.0, 0.0), mu=0.0, lmbda=0.0):
+    def __init__(self, kind, V, coeff, function=None, constant=(0.0, 0.0, 0.0), mu=0.0, lmbda=0.0,
+                 pair=None):
         self.kind, self.V, self.coeff = kind, V, coeff
         self.function, self.constant, self.mu, self.lmbda = function, tuple(constant), mu, lmbda
+        # a load c*f1*f2*v*dx: the two P1 Functions (which one is kappa is
+        # decided by the bilinear form it is assembled with)
+        self.pair = pair
+
+    def with_kappa(self, kappa):
+        """The load c*kappa*f*v*dx of a two-Function load, kappa being the
+        bilinear form's coefficient: DB2_COEFF_P1_KAPPA with f."""
+        from . import _capi
+        if self.pair is None or kappa is None or not any(kappa is g for g in self.pair):
+            raise NotImplementedError("a load with two Functions is provided as kappa*f*v*dx, kappa "
+                                      "being the bilinear form's coefficient (SystemAssembler)")
+        f = self.pair[1] if self.pair[0] is kappa else self.pair[0]
+        return Recognised(self.kind, self.V, _capi.COEFF_P1_KAPPA, f, self.constant)
 
     def c_form(self):
         from . import _capi
@@ -516,6 +530,8 @@ def recognise(form, _kind=None):
     args = form.arguments()
     rank = len(args)
     fs, _ = form.coefficients()
+    if len(fs) == 2 and rank == 1 and _kind is None:
+        return _recognise_pair_load(form, args, fs)
     if len(fs) > 1:
         raise NotImplementedError("forms with more than one Function coefficient are not provided")
     func = fs[0] if fs else None
@@ -607,6 +623,38 @@ def recognise(form, _kind=None):
         return Recognised(lkind, V, _capi.COEFF_CONSTANT, None, tuple(fvec) + (0.0,) * (3 - vs))
 
     raise NotImplementedError("functionals: use assemble() (rank-0 forms)")
+
+
+def _recognise_pair_load(form, args, fs):
+    """c*f1*f2*v*dx with two scalar P1 Functions (the kappa-weighted load
+    kappa*f*v*dx of an adjoint problem)."""
+    from . import _capi
+    for g in fs:
+        if g.function_space().degree() != 1 or g.function_space().value_size() != 1:
+            raise NotImplementedError("coefficients must be scalar P1 Functions")
+    V = args[0]
+    if V.value_size() != 1:
+        raise NotImplementedError("a load with two Functions is provided on scalar spaces")
+    rng = np.random.default_rng(20190404)
+    I = form.integrand()
+    f1, f2 = fs
+
+    def fv(a, b):
+        return {f1: np.full(_NPROBE, a), f2: np.full(_NPROBE, b)}
+
+    env = _env(rng, args, fv(1.0, 1.0))
+    full = I.ev(env)
+    env0 = dict(env, grad={k: np.zeros_like(v) for k, v in env["grad"].items()})
+    if not _close(I.ev(env0), full):
+        raise NotImplementedError("only c*f*g*v*dx loads with two Functions are provided")
+    F1 = full / env["val"][0]
+    if not np.allclose(F1, F1[0], rtol=1e-10):
+        raise NotImplementedError("linear form is not c*f*g*v*dx")
+    for a, b in ((2.0, 1.0), (1.0, 2.0), (3.0, 5.0)):
+        if not _close(I.ev(dict(env, f=fv(a, b))) / env["val"][0], a * b * F1):
+            raise NotImplementedError("the two Functions must enter as a product factor")
+    alpha = _unit_probe(lambda e: I.ev(e), args, fv(1.0, 1.0), grads=False)
+    return Recognised(_capi.FORM_LOAD, V, _capi.COEFF_P1_KAPPA, None, (alpha, 0, 0), pair=(f1, f2))
 
 
 def _unit_probe(ev, args, fv, grads):

@@ -66,8 +66,11 @@ enum db2_coeff_kind {
   DB2_COEFF_CONSTANT = 1,  /* dolfin Constant: constant[] (scalar or vector)*/
   DB2_COEFF_P1 = 2,        /* P1 Function: device array of vertex values     */
   DB2_COEFF_P1_SCALED = 3, /* constant[0] * P1 Function                      */
-  DB2_COEFF_COORD = 4      /* constant[0] * x[i], i = (int)constant[1]
+  DB2_COEFF_COORD = 4,     /* constant[0] * x[i], i = (int)constant[1]
                               (SpatialCoordinate; functionals only)         */
+  DB2_COEFF_P1_KAPPA = 5   /* L = constant[0] * kappa * f * v * dx: f the
+                              load's P1 field, kappa the bilinear form's P1
+                              field (system assembly of kappa*grad.grad)    */
 };
 enum db2_precision {
   DB2_FP64 = 0,            /* geometry, contraction, accumulation in FP64    */
@@ -213,6 +216,20 @@ int db2_pattern_retile(db2_pattern P, int tile_threads, int seg_cap_bytes);
    as they were.  [0, nnodes) restores full assembly.  Natural numbering
    only. */
 int db2_pattern_set_row_range(db2_pattern P, int64_t node_begin, int64_t node_end);
+/* As db2_pattern_set_row_range, and the value and vector arrays the
+   assembly entry points take then hold the row block alone: the CSR rows of
+   nodes [node_begin, node_end) of every component, in global row order
+   (component-major), and their b entries likewise -- the rows a rank owns in
+   DOLFIN's distributed SparsityPattern (dolfin/la/SparsityPattern.cpp:
+   200-255), stored without the rest of the matrix.  Sizes:
+   db2_pattern_row_block_info; the block's row pointers (from 0) and global
+   column indices: db2_pattern_row_block_csr_host.  The adjoint entry points
+   refuse row-block storage (their gradients are whole-CSR arrays); the
+   matrix-free action is unaffected (x and y stay whole vectors).  The plan
+   (incidence records) stays whole on the device. */
+int db2_pattern_set_row_block(db2_pattern P, int64_t node_begin, int64_t node_end);
+int db2_pattern_row_block_info(db2_pattern P, int64_t* nrows, int64_t* nnz);
+int db2_pattern_row_block_csr_host(db2_pattern P, int32_t* rowptr, int32_t* cols);
 
 /* ---- assembly --------------------------------------------------------- */
 /* Assembler::assemble(A, a) (dolfin/fem/Assembler.cpp:52-103) for a bilinear
@@ -277,9 +294,10 @@ int db2_assemble_facets_bc(db2_pattern P, const db2_form* a_ds, const double* wa
 int db2_apply(db2_pattern P, const db2_form* a, const double* w, int precision, const double* x,
               double* y, void* stream);
 /* Vector-Jacobian product of (A(kappa), b(kappa)) for a = kappa grad.grad
-   (P1 kappa) and L = f v dx, or kappa f v dx when L->coeff is
-   DB2_COEFF_P1_SCALED with constant[0] ignored: dkappa[Nv] = sum gA*dA/dkappa
-   + sum gb*db/dkappa.  gA[nnz], gb[N] device (gb may be NULL).  This is the
+   (P1 kappa) and L = f v dx, or the kappa-weighted load
+   constant[0] * kappa f v dx when L->coeff is DB2_COEFF_P1_KAPPA (also
+   DB2_COEFF_P1_SCALED, with constant[0] ignored, for earlier callers):
+   dkappa[Nv] = sum gA*dA/dkappa + sum gb*db/dkappa.  gA[nnz], gb[N] device (gb may be NULL).  This is the
    assembly of UFL's derivative(a, kappa) form (the reference's
    python/test/unit/fem/test_coordinate_derivative.py style check). */
 int db2_vjp_kappa(db2_pattern P, const db2_form* a, const double* kappa, const db2_form* L,

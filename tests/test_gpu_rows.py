@@ -66,3 +66,41 @@ def test_row_partitioned_assembly_equals_full(kind, nranks):
     torch.cuda.synchronize()
     assert torch.equal(A2.values_tensor(), ref_vals)
     assert torch.equal(b2.tensor(), ref_b)
+
+
+@pytest.mark.parametrize("kind", ["p2", "elas", "p1bc", "p1ds", "p1dsbc"])
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_row_blocks_held_alone_equal_full(kind, nranks):
+    """Each rank holds only its row block (shard.RowBlock: its CSR rows and b
+    entries, allocated alone); placed back at their global rows, the blocks
+    are the full assembly bit for bit."""
+    V, a, L, bcs = _problem(kind)
+    A, b = d2.SystemAssembler(a, L, bcs).assemble()
+    ref_vals, ref_b = A.values_tensor().cpu().numpy(), b.get_local()
+    P = A.pattern
+    frp, _ = P.csr_host()
+    nn = V.dim() // V.value_size()
+    cuts = shard.row_partition(P.plan()["inc_ptr"], nranks)
+    vals = np.full(len(ref_vals), np.nan)
+    bv = np.full(len(ref_b), np.nan)
+    try:
+        for r in range(nranks):
+            blk = shard.RowBlock(V, int(cuts[r]), int(cuts[r + 1]))
+            assert blk.vals.numel() < len(ref_vals) or nranks == 1
+            bvals, bb = blk.assemble_system(a, L, bcs)
+            torch.cuda.synchronize()
+            rp, _ = blk.csr_host()
+            bvals, bb = bvals.cpu().numpy(), bb.cpu().numpy()
+            for i, dof in enumerate(blk.dofs()):
+                vals[frp[dof]:frp[dof + 1]] = bvals[rp[i]:rp[i + 1]]
+            bv[blk.dofs()] = bb
+    finally:
+        P.set_row_range(0, nn)
+    assert np.array_equal(vals, ref_vals)
+    assert np.array_equal(bv, ref_b)
+    with pytest.raises(RuntimeError):
+        P.set_row_block(0, nn // 2)
+        try:
+            d2.SystemAssembler(a, L, bcs).assemble(A, b)
+        finally:
+            P.set_row_range(0, nn)

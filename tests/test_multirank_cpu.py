@@ -67,3 +67,54 @@ def test_lpt_balance():
     parts = lpt_assign(w, 8)
     loads = [sum(w[i] for i in p) for p in parts]
     assert max(loads) - min(loads) <= w.max()
+
+
+def _block_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import dolfin_b200 as d2
+        from dolfin_b200 import shard
+        mesh = d2.UnitCubeMesh(3, 3, 3)
+        V = d2.VectorFunctionSpace(mesh, "Lagrange", 2)
+        P = V.pattern()
+        cuts = shard.row_partition(P.plan()["inc_ptr"], world)
+        P.set_row_block(int(cuts[rank]), int(cuts[rank + 1]))
+        nrows, nnz = P.row_block_info()
+        rp, cols = P.row_block_csr_host()
+        dofs = shard.row_block_dofs(V.dim() // 3, 3, int(cuts[rank]), int(cuts[rank + 1]))
+        got = [None] * world
+        dist.all_gather_object(got, (dofs.tolist(), rp.tolist(), cols.tolist(), nrows, nnz))
+        P.set_row_range(0, V.dim() // 3)
+        frp, fcols = P.csr_host()
+        q.put((rank, got, frp.tolist(), fcols.tolist()))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def test_row_blocks_partition_the_csr_two_ranks():
+    """Each rank's row block (its own CSR rows, rowptr from 0, global
+    columns) is exactly the whole pattern's rows of its dofs; together the
+    blocks hold every row once."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_block_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    rank, got, frp, fcols = res[0]
+    frp, fcols = np.array(frp), np.array(fcols)
+    all_dofs = []
+    for dofs, rp, cols, nrows, nnz in got:
+        rp, cols = np.array(rp), np.array(cols)
+        assert len(dofs) == nrows and rp[-1] == nnz == len(cols) and rp[0] == 0
+        for i, d in enumerate(dofs):
+            assert np.array_equal(cols[rp[i]:rp[i + 1]], fcols[frp[d]:frp[d + 1]])
+        all_dofs += dofs
+    assert sorted(all_dofs) == list(range(len(frp) - 1))
