@@ -59,6 +59,7 @@ _SIGS = {
     "db2_mesh_read_xdmf": [C.c_char_p, PP],
     "db2_pattern_set_row_range": [P, C.c_int64, C.c_int64],
     "db2_pattern_set_row_block": [P, C.c_int64, C.c_int64],
+    "db2_tensor_core_status": [P],
     "db2_pattern_row_block_info": [P, P, P],
     "db2_pattern_row_block_csr_host": [P, P, P],
     "db2_mesh_write_xdmf": [P, C.c_char_p, P, C.c_int, C.c_char_p],

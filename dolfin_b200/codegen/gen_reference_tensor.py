@@ -1,0 +1,93 @@
+#!/usr/bin/env python3
+"""Generates ``csrc/generated/ref_tensor.h``: the whole reference tensor of
+kappa*inner(grad(u), grad(v))*dx on P2 tetrahedra with a P1 kappa, as the
+B operand of a tensor-core contraction.
+
+With the barycentric gradients g_a of the affine tetrahedron T and the P1
+kappa = sum_m kappa_m lambda_m (Kirby & Logg's reference tensor x geometry
+tensor factorisation, as in gen_element_rows.py):
+
+    A_ij = sum_m sum_{a<=b} G_(m,ab) R_(m,ab),ij / DEN
+    G_(m,ab) = kappa_m W_ab,   W_ab = |T| g_a.g_b       (the geometry tensor)
+    R_(m,ab),ij = DEN (1/|T|) int_T lambda_m (dphi_i/dlambda_a dphi_j/dlambda_b
+                                             + [a<b] dphi_i/dlambda_b dphi_j/dlambda_a)
+
+R is an integer matrix (40 features x 100 entries of the 10 x 10 element
+matrix, row-major): DEN is the least common denominator of the exact
+rationals, so R is exact in half precision (|R| < 2048) and the only
+rounding of the contraction is in the geometry operand and the FP32 sums.
+
+Run:  python dolfin_b200/codegen/gen_reference_tensor.py   (rewrites the header)
+"""
+from __future__ import annotations
+
+import os
+from math import lcm
+
+import sympy as sp
+
+from gen_element_rows import basis, integrate, lam_symbols
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "..", "csrc", "generated", "ref_tensor.h")
+
+PAIRS = [(a, b) for a in range(4) for b in range(a, 4)]  # the 10 symmetric (a, b)
+
+
+def reference_tensor_p2tet():
+    """(R as a list of 40 rows of 100 ints, DEN)."""
+    L = lam_symbols(3)
+    phi = basis(3, 2)
+    dphi = [[sp.diff(f, L[a]) for a in range(4)] for f in phi]
+    rows = []
+    for m in range(4):
+        for a, b in PAIRS:
+            row = []
+            for i in range(10):
+                for j in range(10):
+                    e = dphi[i][a] * dphi[j][b]
+                    if a != b:
+                        e += dphi[i][b] * dphi[j][a]
+                    row.append(integrate(L[m] * e, 3))
+            rows.append(row)
+    den = 1
+    for row in rows:
+        for v in row:
+            den = lcm(den, int(sp.Rational(v).q))
+    R = [[int(v * den) for v in row] for row in rows]
+    return R, den
+
+
+def main():
+    R, den = reference_tensor_p2tet()
+    big = max(abs(v) for row in R for v in row)
+    assert big < 2048, big
+    lines = [
+        "// Generated by dolfin_b200/codegen/gen_reference_tensor.py -- do not edit.",
+        "// Reference tensor of kappa*inner(grad(u), grad(v))*dx, P2 tetrahedra, P1",
+        "// kappa: A_ij = sum_f G_f R[f][10 i + j] / DEN, f = 10 m + pair(a, b),",
+        "// G_f = kappa_m |T| g_a.g_b, pairs (a <= b) in the order",
+        "// " + " ".join(f"({a},{b})" for a, b in PAIRS) + ".",
+        "#pragma once",
+        "",
+        "namespace db2 {",
+        "namespace gen {",
+        "",
+        f"constexpr int kRefP2TetFeatures = {len(R)};",
+        f"constexpr int kRefP2TetEntries = {len(R[0])};",
+        f"constexpr double kRefP2TetDen = {den}.0;",
+        f"constexpr int kRefP2TetMaxAbs = {big};",
+        "#ifdef __CUDACC__",
+        "// the tensor itself, in constant memory (read once per CTA)",
+        "__constant__ short kRefP2Tet[40][100] = {",
+    ]
+    for row in R:
+        lines.append("    {" + ", ".join(str(v) for v in row) + "},")
+    lines += ["};", "#endif", "", "}  // namespace gen", "}  // namespace db2", ""]
+    with open(OUT, "w") as fh:
+        fh.write("\n".join(lines))
+    print(f"wrote {OUT}: DEN = {den}, max |R| = {big}")
+
+
+if __name__ == "__main__":
+    main()

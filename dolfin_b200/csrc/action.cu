@@ -4,6 +4,9 @@
 #include <cuda_runtime.h>
 
 #include "launch.cuh"
+#include "action_tc.cuh"
+
+#include <algorithm>
 
 namespace db2 {
 namespace dev {
@@ -360,7 +363,42 @@ void run_apply(const Pattern& Pt, const AsmParams& p, const double* x, double* y
   check_cuda("apply gather launch");
 }
 
+// The FP32-contraction action of P2 diffusion on tetrahedra: element actions
+// by the tensor-core kernel (action_tc.cuh), then the same ordered gather.
+template <bool KP1>
+void run_apply_tc(const Pattern& Pt, const AsmParams& p, const double* x, double* y, cudaStream_t s) {
+  const int64_t nc = Pt.V->mesh->nc;
+  const size_t need = size_t(nc) * 10 * sizeof(double);
+  if (Pt.d_cellvals.bytes < need) Pt.d_cellvals.alloc(need);
+  double* ycell = Pt.d_cellvals.as<double>();
+  if (nc > 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_tc_p2<KP1>, kTcM, sizeof(TcSmem));
+    // persistent: at most the resident CTAs (each holds 64 tensor-memory
+    // columns; 8 fit an SM's 512)
+    per_sm = std::min(std::max(per_sm, 1), 8);
+    const int64_t ntiles = (nc + kTcM - 1) / kTcM;
+    const unsigned grid = unsigned(std::min<int64_t>(ntiles, int64_t(sms) * per_sm));
+    k_apply_tc_p2<KP1><<<grid, kTcM, sizeof(TcSmem), s>>>(p, nc, x, ycell);
+    count_launch();
+    check_cuda("tensor-core apply launch");
+  }
+  k_apply_gather<1, 10, true><<<unsigned((p.nnodes + 255) / 256), 256, 0, s>>>(p.inc_ptr, p.inc, p.nnodes,
+                                                                              ycell, y);
+  count_launch();
+  check_cuda("apply gather launch");
+}
+
 }  // namespace dev
+
+int tensor_core_status() {
+  int v = 0;
+  const cudaError_t e = cudaMemcpyFromSymbol(&v, dev::g_tc_status, sizeof(int));
+  if (e != cudaSuccess) fail(DB2_ERR_CUDA, "reading the tensor-core status: %s", cudaGetErrorString(e));
+  return v;
+}
 
 dev::AsmParams make_params(const Pattern& P);
 void pack_vertex_records(const Pattern& P, const double* kappa, const double* f, void* stream);
@@ -380,6 +418,12 @@ void launch_apply(const Pattern& P, const FormArgs& a, int precision, const doub
     if (kp1 && !a.w) fail(DB2_ERR_ARGUMENT, "P1 coefficient field missing");
     p.kappa = a.w;
     pack_vertex_records(P, kp1 ? a.w : nullptr, nullptr, stream);
+    if (fp32 && D == 3 && deg == 2) {
+      // FP32 contraction on the tensor cores
+      if (kp1) dev::run_apply_tc<true>(P, p, x, y, s);
+      else dev::run_apply_tc<false>(P, p, x, y, s);
+      return;
+    }
 #define DB2_AP(D_, P_)                                                                  \
   if (D == D_ && deg == P_) {                                                           \
     if (kp1) {                                                                          \

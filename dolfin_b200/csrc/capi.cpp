@@ -581,6 +581,13 @@ int db2_apply(db2_pattern P, const db2_form* a, const double* w, int precision, 
   });
 }
 
+int db2_tensor_core_status(int* status) {
+  return guard([&] {
+    need(status, "status");
+    *status = db2::tensor_core_status();
+  });
+}
+
 int db2_vjp_kappa(db2_pattern P, const db2_form* a, const double* kappa, const db2_form* L,
                   const double* f, const double* gA, const double* gb, int precision,
                   double* dkappa, void* stream) {

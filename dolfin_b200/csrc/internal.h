@@ -244,6 +244,9 @@ size_t vjp_scratch_doubles(const Pattern& P);
 // Load the adjoint kernels onto the current device (lazy module loading
 // would otherwise do it, allocating, at their first launch).
 void preload_vjp_kernels();
+// 1 if a tensor-core kernel's bounded wait ran out since the process started
+// (its outputs were written as NaN); reads the device flag synchronously.
+int tensor_core_status();
 // Once per device: set up the allocation-free adjoint's fixed scratch array
 // (vjp_noalloc.cu); called by Pattern::ensure_device.
 void noalloc_prepare_device();
