@@ -516,7 +516,7 @@ def dofs_per_cell(w):
     return k_node * (3 if w["kind"] == "elasticity" else 1)
 
 
-def measure_action(w, args, flush, peak, repeats=0):
+def measure_action(w, args, flush, peak, repeats=0, precision="fp64"):
     """Matrix-free action on the workload's form: per-action device time
     (L2 flushed between actions), the roofline numbers, and optionally the
     time of `repeats` back-to-back actions (one event window)."""
@@ -526,9 +526,10 @@ def measure_action(w, args, flush, peak, repeats=0):
     x = torch.randn(V.dim(), dtype=torch.float64, device="cuda",
                     generator=torch.Generator("cuda").manual_seed(7))
     xv, y = d2.Vector(x), d2.Vector(n=V.dim())
+    act = lambda: d2.assemble_action(w["a"], xv, y, precision=precision)
     for _ in range(args.warmup):
-        d2.assemble_action(w["a"], xv, y)
-    ms = float(np.mean(time_steps(lambda: d2.assemble_action(w["a"], xv, y), args.steps, flush)))
+        act()
+    ms = float(np.mean(time_steps(act, args.steps, flush)))
     C, Nv = mesh.num_cells(), mesh.num_vertices()
     k_node = 10 if w["deg"] == 2 else 4
     by = action_bytes(C, k_node, 3, Nv, Nv if w["kind"] == "poisson" else 0, V.dim())
@@ -547,7 +548,7 @@ def measure_action(w, args, flush, peak, repeats=0):
         flush.zero_()
         s.record()
         for _ in range(repeats):
-            d2.assemble_action(w["a"], xv, y)
+            act()
         e.record()
         torch.cuda.synchronize()
         tot = s.elapsed_time(e)
@@ -592,6 +593,18 @@ def extra_config5(args, flush, peak, rank):
            "algorithmic_bytes": by, "setup_s": round(w["setup_s"], 2)}
     out["traffic"], out["traffic_source"] = profiled_traffic("poisson_p2_96")
     out["matrix_free"] = measure_action(w, args, flush, peak, repeats=100)
+    # the FP32-contraction action: reference tensor x geometry tensor on the
+    # tensor cores (tcgen05), against the FP64 action
+    tc = measure_action(w, args, flush, peak, repeats=100, precision="fp32")
+    import dolfin_b200 as d2
+    x = torch.randn(w["V"].dim(), dtype=torch.float64, device="cuda",
+                    generator=torch.Generator("cuda").manual_seed(7))
+    y64 = d2.assemble_action(w["a"], d2.Vector(x)).tensor().clone()
+    y32 = d2.assemble_action(w["a"], d2.Vector(x), precision="fp32").tensor()
+    tc["max_rel_err_vs_fp64"] = float((y32 - y64).abs().max() / y64.abs().max())
+    tc["speedup_vs_fp64"] = round(out["matrix_free"]["ms_per_action"] / tc["ms_per_action"], 3)
+    tc["contraction"] = "tcgen05 kind::f16, two half limbs of the FP64 geometry tensor, FP32 accumulation"
+    out["matrix_free_fp32_tensor_core"] = tc
     del w
     torch.cuda.empty_cache()
     return out
@@ -717,11 +730,12 @@ def run_profile(args):
     import torch
     import dolfin_b200 as d2
     w = setup_workload(args.workload, seed=1, device=None, n_override=args.mesh_n)
-    if args.profile == "action":
+    if args.profile in ("action", "action32"):
         x = torch.randn(w["V"].dim(), dtype=torch.float64, device="cuda",
                         generator=torch.Generator("cuda").manual_seed(3))
         xv, y = d2.Vector(x), d2.Vector(n=w["V"].dim())
-        fn = lambda: d2.assemble_action(w["a"], xv, y)
+        prec = "fp32" if args.profile == "action32" else "fp64"
+        fn = lambda: d2.assemble_action(w["a"], xv, y, precision=prec)
     else:
         fn = lambda: w["S"].assemble(w["A"], w["b"])
     for _ in range(args.warmup + args.steps):
@@ -741,7 +755,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the P2 n=96 and adjoint measurements of the default line")
-    ap.add_argument("--profile", choices=["step", "action"], default=None,
+    ap.add_argument("--profile", choices=["step", "action", "action32"], default=None,
                     help="run only the hot loop (for ncu), print no JSON")
     ap.add_argument("--mesh-n", type=int, default=None, help="mesh size override (with --profile)")
     ap.add_argument("--split", choices=["replicas", "rows"], default="replicas",
