@@ -228,10 +228,10 @@ __global__ void __launch_bounds__(256) k_apply_cells(const AsmParams p, int64_t 
 // measured faster than component planes in incidence order for its three
 // component threads per cell (0.33 ms against 0.46 ms per action, vector P2
 // on UnitCubeMesh(48)).
-template <int BS, int K, bool INC>
+template <int BS, int K, bool INC, typename ST = double>
 __global__ void __launch_bounds__(256) k_apply_gather(const uint32_t* __restrict__ inc_ptr,
                                                       const uint32_t* __restrict__ inc,
-                                                      int64_t nnodes, const double* __restrict__ ycell,
+                                                      int64_t nnodes, const ST* __restrict__ ycell,
                                                       double* __restrict__ y) {
   const int64_t node = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (node >= nnodes) return;
@@ -240,13 +240,13 @@ __global__ void __launch_bounds__(256) k_apply_gather(const uint32_t* __restrict
 #pragma unroll
   for (int c = 0; c < BS; ++c) acc[c] = 0.0;
   if constexpr (INC) {
-    for (uint32_t s = s0; s < s1; ++s) acc[0] += __ldg(ycell + s);
+    for (uint32_t s = s0; s < s1; ++s) acc[0] += double(__ldg(ycell + s));
   } else {
     for (uint32_t s = s0; s < s1; ++s) {
       const uint32_t w = __ldg(inc + s);
-      const double* t = ycell + (size_t(w & 0x0fffffffu) * K + (w >> 28)) * BS;
+      const ST* t = ycell + (size_t(w & 0x0fffffffu) * K + (w >> 28)) * BS;
 #pragma unroll
-      for (int c = 0; c < BS; ++c) acc[c] += __ldg(t + c);
+      for (int c = 0; c < BS; ++c) acc[c] += double(__ldg(t + c));
     }
   }
 #pragma unroll
@@ -368,25 +368,24 @@ void run_apply(const Pattern& Pt, const AsmParams& p, const double* x, double* y
 template <bool KP1>
 void run_apply_tc(const Pattern& Pt, const AsmParams& p, const double* x, double* y, cudaStream_t s) {
   const int64_t nc = Pt.V->mesh->nc;
-  const size_t need = size_t(nc) * 10 * sizeof(double);
+  const size_t need = size_t(nc) * 10 * sizeof(float);
   if (Pt.d_cellvals.bytes < need) Pt.d_cellvals.alloc(need);
-  double* ycell = Pt.d_cellvals.as<double>();
+  float* ycell = Pt.d_cellvals.as<float>();
   if (nc > 0) {
-    int dev = 0, sms = 0, per_sm = 0;
+    int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_tc_p2<KP1>, kTcM, sizeof(TcSmem));
-    // persistent: at most the resident CTAs (each holds 64 tensor-memory
-    // columns; 8 fit an SM's 512)
-    per_sm = std::min(std::max(per_sm, 1), 8);
+    // persistent: the 5 CTAs per SM the launch bounds provide for (registers
+    // <= 102; 5 x 30 KB of shared memory; 5 x 64 of the 512 tensor-memory
+    // columns)
     const int64_t ntiles = (nc + kTcM - 1) / kTcM;
-    const unsigned grid = unsigned(std::min<int64_t>(ntiles, int64_t(sms) * per_sm));
+    const unsigned grid = unsigned(std::min<int64_t>(ntiles, int64_t(sms) * 5));
     k_apply_tc_p2<KP1><<<grid, kTcM, sizeof(TcSmem), s>>>(p, nc, x, ycell);
     count_launch();
     check_cuda("tensor-core apply launch");
   }
-  k_apply_gather<1, 10, true><<<unsigned((p.nnodes + 255) / 256), 256, 0, s>>>(p.inc_ptr, p.inc, p.nnodes,
-                                                                              ycell, y);
+  k_apply_gather<1, 10, true, float><<<unsigned((p.nnodes + 255) / 256), 256, 0, s>>>(p.inc_ptr, p.inc,
+                                                                                     p.nnodes, ycell, y);
   count_launch();
   check_cuda("apply gather launch");
 }

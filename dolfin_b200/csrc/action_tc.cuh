@@ -11,12 +11,13 @@
 // 48).  A tile of 128 cells is one tensor-core product [128 x 80] x [80 x 64]
 // -> FP32 in tensor memory: the geometry operand is computed in FP64 per
 // cell, scaled by a power of two and split into two half-precision limbs
-// (G = h1 + h2 2^-11, 22 significant bits), the second limb's rows of R
+// (G = h1 + h2 2^-11, 22 significant bits; the features themselves in FP32
+// from the FP64 geometry), the second limb's rows of R
 // scaled by 2^-11 (exact in half precision), so the products are exact and
 // the only rounding is the FP32 accumulation (~3e-7 of max |A_K|).  Each
 // thread then reads its cell's 55 entries from tensor memory, forms
-// y_K = A_K x_K in FP32 and writes y_K (FP64) to the cell's incidence
-// slots; the ordered per-row gather of the FP64 action sums them.
+// y_K = A_K x_K in FP32 and writes y_K (FP32) to the cell's incidence
+// slots; the ordered per-row gather sums them in FP64.
 //
 // One CTA = one warpgroup = 128 threads = 128 tensor-memory lanes (thread t
 // <-> cell t of the tile <-> lane t); persistent over tiles.
@@ -53,9 +54,9 @@ struct TcSmem {
 __device__ int g_tc_status = 0;
 
 template <bool KP1>
-__global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int64_t ncells,
+__global__ void __launch_bounds__(kTcM, 5) k_apply_tc_p2(const AsmParams p, int64_t ncells,
                                                        const double* __restrict__ xin,
-                                                       double* __restrict__ ycell) {
+                                                       float* __restrict__ ycell) {
   extern __shared__ __align__(128) unsigned char tc_smem_raw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>(tc_smem_raw);
   const int t = threadIdx.x, warp = t >> 5;
@@ -87,8 +88,8 @@ __global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int6
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int64_t cell = tile * kTcM + t;
     const bool live = cell < ncells;
-    // ---- geometry operand (FP64), two half limbs ----------------------------
-    __half h[kTcK];
+    // ---- geometry operand: FP64 geometry, FP32 features, two half limbs ------
+    uint32_t hp[kTcK / 2];  // packed half pairs, k = 2i, 2i + 1
     float xv[10];
     int e = 0;
     if (live) {
@@ -100,49 +101,51 @@ __global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int6
         double f;
         load_vertex<3, false>(p, v[a], x[a], kap[a], f);
       }
-      Geometry<3> Gm;
-      geometry(x, Gm);
-      double W[10], km[4];
-      double wmax = 0.0, kmax = 0.0;
-      int q = 0;
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = a; b < 4; ++b, ++q) {
-          W[q] = Gm.s * ndot<3>(Gm, a, b);  // |K| g_a.g_b
-          wmax = fmax(wmax, fabs(W[q]));
-        }
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        km[m] = KP1 ? p.kscale * kap[m] : p.kscale;
-        kmax = fmax(kmax, fabs(km[m]));
-      }
-      frexp(wmax * kmax, &e);  // |G| < 2^e
-#pragma unroll
-      for (int m = 0; m < 4; ++m)
-#pragma unroll
-        for (int r = 0; r < 10; ++r) {
-          const double g = ldexp(km[m] * W[r], -e);
-          const __half h1 = __double2half(g);
-          h[m * 10 + r] = h1;
-          h[kTcF + m * 10 + r] = __double2half((g - double(__half2float(h1))) * 2048.0);
-        }
 #pragma unroll
       for (int j = 0; j < 10; ++j) {
         const uint32_t node = j < 4 ? v[j] : __ldg(p.cell_nodes + size_t(cell) * 10 + j);
         xv[j] = float(__ldg(xin + node));
       }
+      Geometry<3> Gm;
+      geometry(x, Gm);
+      float W[10], km[4];
+      float wmax = 0.f, kmax = 0.f;
+      int q = 0;
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = a; b < 4; ++b, ++q) {
+          W[q] = float(Gm.s * ndot<3>(Gm, a, b));  // |K| g_a.g_b
+          wmax = fmaxf(wmax, fabsf(W[q]));
+        }
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        km[m] = float(KP1 ? p.kscale * kap[m] : p.kscale);
+        kmax = fmaxf(kmax, fabsf(km[m]));
+      }
+      // |G| < 2^e; the operand is G 2^-e (a power of two: exact)
+      frexpf(wmax * kmax, &e);
+      e = max(-120, min(120, e));
+      const float sc = __int_as_float((127 - e) << 23);
+      float g[kTcF];
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int r = 0; r < 10; ++r) g[m * 10 + r] = km[m] * W[r] * sc;
+#pragma unroll
+      for (int i = 0; i < kTcF / 2; ++i) {
+        const __half2 h1 = __floats2half2_rn(g[2 * i], g[2 * i + 1]);
+        const float2 back = __half22float2(h1);
+        const __half2 h2 = __floats2half2_rn((g[2 * i] - back.x) * 2048.f, (g[2 * i + 1] - back.y) * 2048.f);
+        hp[i] = *reinterpret_cast<const uint32_t*>(&h1);
+        hp[kTcF / 2 + i] = *reinterpret_cast<const uint32_t*>(&h2);
+      }
     } else {
 #pragma unroll
-      for (int k = 0; k < kTcK; ++k) h[k] = __float2half_rn(0.f);
+      for (int i = 0; i < kTcK / 2; ++i) hp[i] = 0u;
     }
 #pragma unroll
-    for (int c = 0; c < kTcChunks; ++c) {
-      auto pk = [&](int k) {
-        return uint32_t(__half_as_ushort(h[k])) | (uint32_t(__half_as_ushort(h[k + 1])) << 16);
-      };
-      S.a[c][t] = make_uint4(pk(8 * c), pk(8 * c + 2), pk(8 * c + 4), pk(8 * c + 6));
-    }
+    for (int c = 0; c < kTcChunks; ++c) S.a[c][t] = make_uint4(hp[4 * c], hp[4 * c + 1], hp[4 * c + 2], hp[4 * c + 3]);
     // the tile's rows (generic proxy) -> the tensor core (async proxy); the
     // previous tile's tensor-memory reads are complete before the product
     umma::fence_async_smem();
@@ -163,7 +166,7 @@ __global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int6
     if (!done) {
       if (t == 0) atomicExch(&g_tc_status, 1);
       if (live)
-        for (int j = 0; j < 10; ++j) ycell[__ldg(p.cell_inc + size_t(cell) * 10 + j)] = __longlong_as_double(-1ll);
+        for (int j = 0; j < 10; ++j) ycell[__ldg(p.cell_inc + size_t(cell) * 10 + j)] = __int_as_float(-1);
       break;
     }
     umma::fence_after_sync();
@@ -181,9 +184,9 @@ __global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int6
           y[i] = fmaf(acc[n], xv[j], y[i]);
           if (j != i) y[j] = fmaf(acc[n], xv[i], y[j]);
         }
-      const double sc = ldexp(1.0, e) / gen::kRefP2TetDen;
+      const float sc = __int_as_float((127 + e) << 23) * (1.f / float(gen::kRefP2TetDen));
 #pragma unroll
-      for (int j = 0; j < 10; ++j) ycell[__ldg(p.cell_inc + size_t(cell) * 10 + j)] = double(y[j]) * sc;
+      for (int j = 0; j < 10; ++j) ycell[__ldg(p.cell_inc + size_t(cell) * 10 + j)] = y[j] * sc;
     }
   }
   umma::fence_before_sync();
