@@ -58,6 +58,34 @@ def reference_tensor_p2tet():
     return R, den
 
 
+def b_operand_text(R, nrows=64):
+    """The tensor-core B operand, ready to copy to shared memory: row n =
+    entry (i <= j) of the 10 x 10 element matrix (row-major over i <= j,
+    padded to 64 rows), K = 80 = two limbs of the 40 features (the second
+    limb's R scaled by 2^-11, exact), in the canonical K-major layout
+    without swizzle -- 16-byte cells [k / 8][n] of 8 halves -- as uint4."""
+    import numpy as np
+    pairs = [(i, j) for i in range(10) for j in range(i, 10)]
+    B = np.zeros((nrows, 80), np.float16)
+    for n, (i, j) in enumerate(pairs):
+        for k in range(80):
+            v = R[k % 40][10 * i + j] * (1.0 if k < 40 else 2.0 ** -11)
+            B[n, k] = np.float16(v)
+            assert float(B[n, k]) == v  # exact in half precision
+    words = B.view(np.uint16).astype(np.uint32)
+    out = ["// B operand of the tensor-core action (see gen_reference_tensor.py)",
+           f"__device__ const uint4 kRefP2TetB[10][{nrows}] = {{"]
+    for c in range(10):
+        cells = []
+        for n in range(nrows):
+            w = words[n, 8 * c:8 * c + 8]
+            u = [int(w[2 * q]) | (int(w[2 * q + 1]) << 16) for q in range(4)]
+            cells.append("{" + ", ".join(f"0x{x:08x}u" for x in u) + "}")
+        out.append("    {" + ", ".join(cells) + "},")
+    out.append("};")
+    return out
+
+
 def main():
     R, den = reference_tensor_p2tet()
     big = max(abs(v) for row in R for v in row)
@@ -83,7 +111,9 @@ def main():
     ]
     for row in R:
         lines.append("    {" + ", ".join(str(v) for v in row) + "},")
-    lines += ["};", "#endif", "", "}  // namespace gen", "}  // namespace db2", ""]
+    lines += ["};", ""]
+    lines += b_operand_text(R)
+    lines += ["#endif", "", "}  // namespace gen", "}  // namespace db2", ""]
     with open(OUT, "w") as fh:
         fh.write("\n".join(lines))
     print(f"wrote {OUT}: DEN = {den}, max |R| = {big}")

@@ -54,27 +54,16 @@ struct TcSmem {
 __device__ int g_tc_status = 0;
 
 template <bool KP1>
-__global__ void __launch_bounds__(kTcM, 5) k_apply_tc_p2(const AsmParams p, int64_t ncells,
+__global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int64_t ncells,
                                                        const double* __restrict__ xin,
                                                        float* __restrict__ ycell) {
   extern __shared__ __align__(128) unsigned char tc_smem_raw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>(tc_smem_raw);
   const int t = threadIdx.x, warp = t >> 5;
-  // B: entry n = (i <= j) row-major, limb-2 rows scaled by 2^-11
-  for (int idx = t; idx < kTcN * kTcK; idx += kTcM) {
-    const int n = idx / kTcK, k = idx - n * kTcK;
-    float v = 0.f;
-    if (n < kTcEntries) {
-      int i = 0, r = n;
-      while (r >= 10 - i) {
-        r -= 10 - i;
-        ++i;
-      }
-      const int j = i + r;
-      v = float(gen::kRefP2Tet[k % kTcF][10 * i + j]) * (k < kTcF ? 1.f : 1.f / 2048.f);
-    }
-    reinterpret_cast<__half*>(&S.b[k >> 3][n])[k & 7] = __float2half_rn(v);
-  }
+  // B: the generated operand (entry n = (i <= j) row-major, limb-2 rows
+  // scaled by 2^-11), copied to shared memory
+  for (int idx = t; idx < kTcChunks * kTcN; idx += kTcM)
+    (&S.b[0][0])[idx] = __ldg(&gen::kRefP2TetB[0][0] + idx);
   const uint32_t bar = umma::smem_u32(&S.bar);
   if (t == 0) umma::mbar_init(bar, 1);
   if (warp == 0) umma::tmem_alloc(umma::smem_u32(&S.tmem), kTcN);
@@ -85,27 +74,48 @@ __global__ void __launch_bounds__(kTcM, 5) k_apply_tc_p2(const AsmParams p, int6
   constexpr uint32_t idesc = umma::idesc_f16_f32(kTcM, kTcN);
   const int64_t ntiles = (ncells + kTcM - 1) / kTcM;
   uint32_t phase = 0;
+  // the cell data of a thread's next tile is loaded one tile ahead: vertex
+  // ids, edge nodes and incidence slots do not depend on the arithmetic
+  const int64_t stride = int64_t(gridDim.x) * kTcM;
+  uint4 nv4 = make_uint4(0, 0, 0, 0);
+  uint32_t nnode[6] = {0, 0, 0, 0, 0, 0}, ninc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  auto prefetch = [&](int64_t c) {
+    if (c < ncells) {
+      nv4 = __ldg(reinterpret_cast<const uint4*>(p.cells) + c);
+#pragma unroll
+      for (int j = 0; j < 6; ++j) nnode[j] = __ldg(p.cell_nodes + size_t(c) * 10 + 4 + j);
+#pragma unroll
+      for (int j = 0; j < 10; ++j) ninc[j] = __ldg(p.cell_inc + size_t(c) * 10 + j);
+    }
+  };
+  prefetch(int64_t(blockIdx.x) * kTcM + t);
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int64_t cell = tile * kTcM + t;
     const bool live = cell < ncells;
+    const uint4 v4 = nv4;
+    uint32_t nodes[10], slot[10];
+    nodes[0] = v4.x;
+    nodes[1] = v4.y;
+    nodes[2] = v4.z;
+    nodes[3] = v4.w;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) nodes[4 + j] = nnode[j];
+#pragma unroll
+    for (int j = 0; j < 10; ++j) slot[j] = ninc[j];
+    prefetch(cell + stride);
     // ---- geometry operand: FP64 geometry, FP32 features, two half limbs ------
     uint32_t hp[kTcK / 2];  // packed half pairs, k = 2i, 2i + 1
     float xv[10];
     int e = 0;
     if (live) {
-      const uint4 v4 = __ldg(reinterpret_cast<const uint4*>(p.cells) + cell);
-      const uint32_t v[4] = {v4.x, v4.y, v4.z, v4.w};
       double x[4][3], kap[4];
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
         double f;
-        load_vertex<3, false>(p, v[a], x[a], kap[a], f);
+        load_vertex<3, false>(p, nodes[a], x[a], kap[a], f);
       }
 #pragma unroll
-      for (int j = 0; j < 10; ++j) {
-        const uint32_t node = j < 4 ? v[j] : __ldg(p.cell_nodes + size_t(cell) * 10 + j);
-        xv[j] = float(__ldg(xin + node));
-      }
+      for (int j = 0; j < 10; ++j) xv[j] = float(__ldg(xin + nodes[j]));
       Geometry<3> Gm;
       geometry(x, Gm);
       float W[10], km[4];
@@ -166,7 +176,7 @@ __global__ void __launch_bounds__(kTcM, 5) k_apply_tc_p2(const AsmParams p, int6
     if (!done) {
       if (t == 0) atomicExch(&g_tc_status, 1);
       if (live)
-        for (int j = 0; j < 10; ++j) ycell[__ldg(p.cell_inc + size_t(cell) * 10 + j)] = __int_as_float(-1);
+        for (int j = 0; j < 10; ++j) ycell[slot[j]] = __int_as_float(-1);
       break;
     }
     umma::fence_after_sync();
@@ -186,7 +196,7 @@ __global__ void __launch_bounds__(kTcM, 5) k_apply_tc_p2(const AsmParams p, int6
         }
       const float sc = __int_as_float((127 + e) << 23) * (1.f / float(gen::kRefP2TetDen));
 #pragma unroll
-      for (int j = 0; j < 10; ++j) ycell[__ldg(p.cell_inc + size_t(cell) * 10 + j)] = y[j] * sc;
+      for (int j = 0; j < 10; ++j) ycell[slot[j]] = y[j] * sc;
     }
   }
   umma::fence_before_sync();
