@@ -375,11 +375,11 @@ void run_apply_tc(const Pattern& Pt, const AsmParams& p, const double* x, double
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // persistent: the 4 CTAs per SM the launch bounds provide for (registers
-    // <= 128; 4 x 30 KB of shared memory; 4 x 64 of the 512 tensor-memory
+    // persistent: the 5 CTAs per SM the launch bounds provide for (registers
+    // <= 102; 5 x 30 KB of shared memory; 5 x 64 of the 512 tensor-memory
     // columns)
     const int64_t ntiles = (nc + kTcM - 1) / kTcM;
-    const unsigned grid = unsigned(std::min<int64_t>(ntiles, int64_t(sms) * 4));
+    const unsigned grid = unsigned(std::min<int64_t>(ntiles, int64_t(sms) * 5));
     k_apply_tc_p2<KP1><<<grid, kTcM, sizeof(TcSmem), s>>>(p, nc, x, ycell);
     count_launch();
     check_cuda("tensor-core apply launch");

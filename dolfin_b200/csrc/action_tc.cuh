@@ -54,7 +54,7 @@ struct TcSmem {
 __device__ int g_tc_status = 0;
 
 template <bool KP1>
-__global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int64_t ncells,
+__global__ void __launch_bounds__(kTcM, 5) k_apply_tc_p2(const AsmParams p, int64_t ncells,
                                                        const double* __restrict__ xin,
                                                        float* __restrict__ ycell) {
   extern __shared__ __align__(128) unsigned char tc_smem_raw[];
@@ -75,17 +75,16 @@ __global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int6
   const int64_t ntiles = (ncells + kTcM - 1) / kTcM;
   uint32_t phase = 0;
   // the cell data of a thread's next tile is loaded one tile ahead: vertex
-  // ids, edge nodes and incidence slots do not depend on the arithmetic
+  // ids and edge nodes do not depend on the arithmetic (the incidence slots
+  // are loaded where they are used: 5 CTAs per SM need <= 102 registers)
   const int64_t stride = int64_t(gridDim.x) * kTcM;
   uint4 nv4 = make_uint4(0, 0, 0, 0);
-  uint32_t nnode[6] = {0, 0, 0, 0, 0, 0}, ninc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  uint32_t nnode[6] = {0, 0, 0, 0, 0, 0};
   auto prefetch = [&](int64_t c) {
     if (c < ncells) {
       nv4 = __ldg(reinterpret_cast<const uint4*>(p.cells) + c);
 #pragma unroll
       for (int j = 0; j < 6; ++j) nnode[j] = __ldg(p.cell_nodes + size_t(c) * 10 + 4 + j);
-#pragma unroll
-      for (int j = 0; j < 10; ++j) ninc[j] = __ldg(p.cell_inc + size_t(c) * 10 + j);
     }
   };
   prefetch(int64_t(blockIdx.x) * kTcM + t);
@@ -93,15 +92,13 @@ __global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int6
     const int64_t cell = tile * kTcM + t;
     const bool live = cell < ncells;
     const uint4 v4 = nv4;
-    uint32_t nodes[10], slot[10];
+    uint32_t nodes[10];
     nodes[0] = v4.x;
     nodes[1] = v4.y;
     nodes[2] = v4.z;
     nodes[3] = v4.w;
 #pragma unroll
     for (int j = 0; j < 6; ++j) nodes[4 + j] = nnode[j];
-#pragma unroll
-    for (int j = 0; j < 10; ++j) slot[j] = ninc[j];
     prefetch(cell + stride);
     // ---- geometry operand: FP64 geometry, FP32 features, two half limbs ------
     uint32_t hp[kTcK / 2];  // packed half pairs, k = 2i, 2i + 1
@@ -176,7 +173,7 @@ __global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int6
     if (!done) {
       if (t == 0) atomicExch(&g_tc_status, 1);
       if (live)
-        for (int j = 0; j < 10; ++j) ycell[slot[j]] = __int_as_float(-1);
+        for (int j = 0; j < 10; ++j) ycell[__ldg(p.cell_inc + size_t(cell) * 10 + j)] = __int_as_float(-1);
       break;
     }
     umma::fence_after_sync();
@@ -196,7 +193,7 @@ __global__ void __launch_bounds__(kTcM, 4) k_apply_tc_p2(const AsmParams p, int6
         }
       const float sc = __int_as_float((127 + e) << 23) * (1.f / float(gen::kRefP2TetDen));
 #pragma unroll
-      for (int j = 0; j < 10; ++j) ycell[slot[j]] = y[j] * sc;
+      for (int j = 0; j < 10; ++j) ycell[__ldg(p.cell_inc + size_t(cell) * 10 + j)] = y[j] * sc;
     }
   }
   umma::fence_before_sync();
