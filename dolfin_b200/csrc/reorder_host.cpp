@@ -187,6 +187,13 @@ std::vector<int32_t> rcm_node_order(const Space& V) {
         }
       }
       color[u] = BLACK;
+      // Tie rule: the same call on the same sequence (a std::deque block in
+      // Set insertion order) as Boost, so equal degrees end where libstdc++'s
+      // std::sort leaves them.  For blocks of at most 16 nodes (every block
+      // of the unit square and cube meshes, P1 and P2, started from a
+      // pseudo-peripheral node) that sort is an insertion sort, which is
+      // stable: ties stay in Set insertion order, whatever the library's
+      // introsort would do with longer blocks.
       std::sort(Q.begin() + begin, Q.end(), less_degree);
     }
   }
