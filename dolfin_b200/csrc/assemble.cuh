@@ -766,19 +766,27 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
       rslot[i] = r.slot(regcol(i));
       rsum[i] += double(out[regcol(i)]);
     }
+    // The slots of one incidence are distinct (the cell's nodes are distinct
+    // columns of the row), so every segment load of the incidence is issued
+    // before its first store: one shared-memory round trip per incidence
+    // rather than one per column, which the compiler cannot arrange itself
+    // (it cannot see that the addresses differ).
     const uint32_t fm = FIRSTF ? r.first_mask() : 0u;
+    auto in_reg = [&](int j) {
+      bool f = false;
+#pragma unroll
+      for (int i = 0; i < NREG; ++i) f = f || j == regcol(i);
+      return f;
+    };
+    double o[E::K];
 #pragma unroll
     for (int j = 0; j < E::K; ++j) {
-      bool in_reg = false;
-#pragma unroll
-      for (int i = 0; i < NREG; ++i) in_reg = in_reg || j == regcol(i);
-      if (!in_reg) {
-        double* a = my + r.slot(j);
-        double o = 0.0;
-        if (!(fm >> j & 1u)) o = *a;  // first touch: no load
-        *a = o + double(out[j]);
-      }
+      o[j] = 0.0;
+      if (!in_reg(j) && !(fm >> j & 1u)) o[j] = my[r.slot(j)];  // first touch: no load
     }
+#pragma unroll
+    for (int j = 0; j < E::K; ++j)
+      if (!in_reg(j)) my[r.slot(j)] = o[j] + double(out[j]);
   }
   if (cnt) {
 #pragma unroll
@@ -788,6 +796,24 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
     }
   }
   bpart[u] = bsum;
+}
+
+// Bulk copy shared -> global (cp.async.bulk, no tensor map): both addresses
+// 16-byte aligned, bytes a multiple of 16.  Completion of the reads of the
+// shared source is awaited by bulk_wait_read; the global writes are
+// performed before the kernel completes.
+__device__ __forceinline__ void bulk_fence() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_store(double* gdst, const double* ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n\t"
+               "cp.async.bulk.commit_group;"
+               :
+               : "l"(gdst), "r"(static_cast<uint32_t>(__cvta_generic_to_shared(ssrc))), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
 // One tile: rows [t.n0, t.n1) of test component t.comp.  `acc` holds the
@@ -804,16 +830,25 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
   constexpr int BS = FORM == FORM_ELAS ? D : 1;
   const int32_t r0 = __ldg(p.node_rowptr + t.n0), r1 = __ldg(p.node_rowptr + t.n1);
   const int seg = BS * (r1 - r0);
-  double* bpart = acc + seg;
+  double* dst = p.vals + int64_t(t.comp) * p.vstride + int64_t(BS) * r0 - p.vbase;
+  // The segment is staged at the address parity (mod 16 bytes) of its
+  // destination, so that its 16-byte-aligned middle leaves shared memory by
+  // one bulk copy (the launch gives one double of slack for the shift).
+  const int sh = int((reinterpret_cast<uintptr_t>(dst) >> 3) & 1u);
+  double* segm = acc + sh;
+  double* bpart = segm + seg;
   const int units = (t.n1 - t.n0) * BS;
   if (int(threadIdx.x) < units) {
     // tiles never mix vertex and edge nodes (the host cuts P2 tiles at the
     // first edge node), so the row kind is uniform over the block
     if (P == 1 || t.n0 < p.nverts)
-      row_unit<D, P, FORM, KP1, LOADM, CT, 1, ESC>(p, t, acc, bpart, r0, int(threadIdx.x));
+      row_unit<D, P, FORM, KP1, LOADM, CT, 1, ESC>(p, t, segm, bpart, r0, int(threadIdx.x));
     else if constexpr (P == 2)
-      row_unit<D, P, FORM, KP1, LOADM, CT, 2, ESC>(p, t, acc, bpart, r0, int(threadIdx.x));
+      row_unit<D, P, FORM, KP1, LOADM, CT, 2, ESC>(p, t, segm, bpart, r0, int(threadIdx.x));
   }
+  // the segment's generic-proxy writes are made visible to the bulk copy
+  // (async proxy) by this fence and the barrier
+  bulk_fence();
   __syncthreads();
   if constexpr (LOADM != LOAD_NONE) {
     // b of each row: its trial blocks' partials in block order
@@ -825,11 +860,19 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
       *bp = p.add_values ? *bp + s : s;
     }
   }
-  double* dst = p.vals + int64_t(t.comp) * p.vstride + int64_t(BS) * r0 - p.vbase;
   if (p.add_values) {
-    for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] += acc[i];
+    for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] += segm[i];
   } else {
-    for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] = acc[i];
+    // an unaligned first and last double by plain stores, the rest (16-byte
+    // aligned at both ends, a multiple of 16 bytes) by one bulk copy that
+    // thread 0 issues and waits to have read before the segment is reused
+    const int nb = seg > sh ? (seg - sh) & ~1 : 0;
+    if (threadIdx.x == 0 && nb > 0) bulk_store(dst + sh, segm + sh, uint32_t(nb) * 8u);
+    if (threadIdx.x == blockDim.x - 1) {
+      if (sh && seg > 0) dst[0] = segm[0];
+      if (seg > sh + nb) dst[seg - 1] = segm[seg - 1];
+    }
+    if (threadIdx.x == 0 && nb > 0) bulk_wait_read();
   }
   __syncthreads();
 }
@@ -869,7 +912,7 @@ constexpr int tile_maxnreg() {
 // (a separate instantiation, so that well-numbered meshes pay nothing).
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, bool ESC>
 __global__ void __maxnreg__((tile_maxnreg<P, FORM, CT>())) k_assemble(const AsmParams p) {
-  extern __shared__ double acc[];
+  extern __shared__ __align__(16) double acc[];
   tile_body<D, P, FORM, KP1, LOADM, CT, ESC>(p, p.tiles[blockIdx.x], acc);
 }
 

@@ -59,7 +59,7 @@ template <typename CT>
 __global__ void __maxnreg__(DB2_BATCH_MAXNREG) k_batch(const BatchMember* __restrict__ members,
                                                            const BatchTile* __restrict__ tiles,
                                                            int ntiles, unsigned int* counter) {
-  extern __shared__ double acc[];
+  extern __shared__ __align__(16) double acc[];
   __shared__ int next;
   for (;;) {
     if (threadIdx.x == 0) next = int(atomicAdd(counter, 1u));
@@ -227,7 +227,7 @@ int db2_batch_create(int count, const db2_pattern* patterns, const db2_form* for
       };
       std::stable_sort(B.tiles.begin(), B.tiles.end(),
                        [&](const dev::BatchTile& a, const dev::BatchTile& b) { return work(a) > work(b); });
-      B.smem = max_seg * 8 + B.threads * 8;
+      B.smem = max_seg * 8 + B.threads * 8 + 16;  // + alignment slack of tile_body
       int dev_id = 0, nsm = 0;
       cudaGetDevice(&dev_id);
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev_id);
