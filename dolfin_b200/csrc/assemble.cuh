@@ -665,14 +665,20 @@ __device__ __forceinline__ double load_row(const AsmParams& p, const Geometry<D>
 
 // One row unit (node row, trial block e) of a tile whose rows are all vertex
 // nodes (NFIX = 1 fixed vertex) or all edge nodes (NFIX = 2).
-template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int NFIX, bool ESC>
+// Variant flags of the tile kernel (separate instantiations, so that the
+// common case pays for neither): records with escaped vertex offsets, and
+// Dirichlet data (without it the row walk carries no boundary-condition state).
+enum { VAR_ESC = 1, VAR_BC = 2 };
+
+template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int NFIX, int VAR>
 __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, double* acc,
                                          double* bpart, int32_t r0, int u) {
   using E = El<D, P>;
   constexpr int BS = FORM == FORM_ELAS ? D : 1;
   constexpr bool FP1 = LOADM == LOAD_P1 || LOADM == LOAD_KP1;
   constexpr bool vertex = NFIX == 1;
-  const bool bc = p.bc_flags != nullptr;
+  constexpr bool ESC = (VAR & VAR_ESC) != 0;
+  const bool bc = (VAR & VAR_BC) != 0 && p.bc_flags != nullptr;
   const uint32_t node = t.n0 + u / BS;
   const int e = u % BS;
   const int32_t ra = __ldg(p.node_rowptr + node);
@@ -825,7 +831,7 @@ __device__ __forceinline__ void bulk_wait_read() {
 // per cell: a Dirichlet row keeps only 1 on its diagonal and contributes g_i
 // to b; other rows move their Dirichlet-column entries to b (b_i -= A_ij g_j)
 // and zero them.
-template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, bool ESC = false>
+template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int VAR = VAR_BC>
 __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, double* acc) {
   constexpr int BS = FORM == FORM_ELAS ? D : 1;
   const int32_t r0 = __ldg(p.node_rowptr + t.n0), r1 = __ldg(p.node_rowptr + t.n1);
@@ -842,9 +848,9 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
     // tiles never mix vertex and edge nodes (the host cuts P2 tiles at the
     // first edge node), so the row kind is uniform over the block
     if (P == 1 || t.n0 < p.nverts)
-      row_unit<D, P, FORM, KP1, LOADM, CT, 1, ESC>(p, t, segm, bpart, r0, int(threadIdx.x));
+      row_unit<D, P, FORM, KP1, LOADM, CT, 1, VAR>(p, t, segm, bpart, r0, int(threadIdx.x));
     else if constexpr (P == 2)
-      row_unit<D, P, FORM, KP1, LOADM, CT, 2, ESC>(p, t, segm, bpart, r0, int(threadIdx.x));
+      row_unit<D, P, FORM, KP1, LOADM, CT, 2, VAR>(p, t, segm, bpart, r0, int(threadIdx.x));
   }
   // the segment's generic-proxy writes are made visible to the bulk copy
   // (async proxy) by this fence and the barrier
@@ -888,7 +894,10 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
 // fixed vertices reloaded) take 96 too: 1.20 ms against 1.35 at 88.  The
 // FP32-contraction rows keep fewer
 // values live and take 80 (12 CTAs): 1.03-1.05x their time at 96 on the
-// elasticity and P1 workloads, no change on P2 n=96.
+// elasticity and P1 workloads, no change on P2 n=96.  The instantiations
+// without Dirichlet data fit lower caps without spills (P2 88, elasticity
+// 80) but are no faster there: P2 n=96 1.042-1.050 ms at 88 and 96,
+// elasticity n=48 1.041 at 80 against 1.006 at 96.
 #ifndef DB2_TILE_MAXNREG_P1
 #define DB2_TILE_MAXNREG_P1 96
 #endif
@@ -908,12 +917,12 @@ constexpr int tile_maxnreg() {
          : P == 1            ? DB2_TILE_MAXNREG_P1
                              : DB2_TILE_MAXNREG_P2;
 }
-// ESC: the pattern has records whose vertex offsets did not fit 16 bits
-// (a separate instantiation, so that well-numbered meshes pay nothing).
-template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, bool ESC>
+// VAR: VAR_ESC when the pattern has records whose vertex offsets did not fit
+// 16 bits, VAR_BC when the call has Dirichlet data.
+template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int VAR>
 __global__ void __maxnreg__((tile_maxnreg<P, FORM, CT>())) k_assemble(const AsmParams p) {
   extern __shared__ __align__(16) double acc[];
-  tile_body<D, P, FORM, KP1, LOADM, CT, ESC>(p, p.tiles[blockIdx.x], acc);
+  tile_body<D, P, FORM, KP1, LOADM, CT, VAR>(p, p.tiles[blockIdx.x], acc);
 }
 
 }  // namespace dev

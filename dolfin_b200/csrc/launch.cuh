@@ -71,10 +71,13 @@ inline SideStreams& side_streams() {
 // alone below the SM's residency limits.
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT>
 void run_assemble(const AsmParams& p, const LaunchCfg& cfg) {
-  auto kern = cfg.escapes ? k_assemble<D, P, FORM, KP1, LOADM, CT, true>
-                          : k_assemble<D, P, FORM, KP1, LOADM, CT, false>;
-  static unsigned long long configured[2] = {0, 0};
-  allow_dynamic_smem(kern, configured[cfg.escapes ? 1 : 0]);
+  const int var = (cfg.escapes ? VAR_ESC : 0) | (p.bc_flags ? VAR_BC : 0);
+  auto kern = var == 0         ? k_assemble<D, P, FORM, KP1, LOADM, CT, 0>
+              : var == VAR_ESC ? k_assemble<D, P, FORM, KP1, LOADM, CT, VAR_ESC>
+              : var == VAR_BC  ? k_assemble<D, P, FORM, KP1, LOADM, CT, VAR_BC>
+                               : k_assemble<D, P, FORM, KP1, LOADM, CT, VAR_ESC | VAR_BC>;
+  static unsigned long long configured[4] = {0, 0, 0, 0};
+  allow_dynamic_smem(kern, configured[var]);
   const auto& cb = *cfg.class_begin;
   const int ncls = int(cb.size()) - 1;
   const bool fork = DB2_CLASS_STREAMS && ncls > 1 && ncls <= SideStreams::kMax;
