@@ -671,7 +671,7 @@ __device__ __forceinline__ double load_row(const AsmParams& p, const Geometry<D>
 enum { VAR_ESC = 1, VAR_BC = 2 };
 
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int NFIX, int VAR>
-__device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, double* acc,
+__device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, CT* acc,
                                          double* bpart, int32_t r0, int u) {
   using E = El<D, P>;
   constexpr int BS = FORM == FORM_ELAS ? D : 1;
@@ -683,7 +683,7 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
   const int e = u % BS;
   const int32_t ra = __ldg(p.node_rowptr + node);
   const int32_t L = __ldg(p.node_rowptr + node + 1) - ra;
-  double* my = acc + BS * (ra - r0) + e * L;
+  CT* my = acc + BS * (ra - r0) + e * L;
   const uint32_t i0 = __ldg(p.inc_ptr + node);
   const uint32_t cnt = __ldg(p.inc_ptr + node + 1) - i0;
   const uint32_t rbase = __ldg(p.rec_goff + (node >> 5)) + (node & 31u);
@@ -715,7 +715,7 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
   // elasticity n=48 1.20 against 1.28).
   constexpr bool FIRSTF = NFIX == 2;
   if (!FIRSTF || cnt == 0)
-    for (int32_t k = 0; k < L; ++k) my[k] = 0.0;
+    for (int32_t k = 0; k < L; ++k) my[k] = CT(0);
   // The row node is relabelled local node 0 (vertex) or K-1 (edge (0,1)),
   // and an edge's end vertices are local nodes 0 and 1: these NREG columns
   // are the same for every incidence, so they are summed in registers (in
@@ -784,21 +784,21 @@ __device__ __forceinline__ void row_unit(const AsmParams& p, const Tile& t, doub
       for (int i = 0; i < NREG; ++i) f = f || j == regcol(i);
       return f;
     };
-    double o[E::K];
+    CT o[E::K];
 #pragma unroll
     for (int j = 0; j < E::K; ++j) {
-      o[j] = 0.0;
+      o[j] = CT(0);
       if (!in_reg(j) && !(fm >> j & 1u)) o[j] = my[r.slot(j)];  // first touch: no load
     }
 #pragma unroll
     for (int j = 0; j < E::K; ++j)
-      if (!in_reg(j)) my[r.slot(j)] = o[j] + double(out[j]);
+      if (!in_reg(j)) my[r.slot(j)] = o[j] + out[j];
   }
   if (cnt) {
 #pragma unroll
     for (int i = 0; i < NREG; ++i) {
-      if (FIRSTF) my[rslot[i]] = 0.0 + rsum[i];  // no other write reaches these slots
-      else my[rslot[i]] += rsum[i];
+      if (FIRSTF) my[rslot[i]] = CT(0.0 + rsum[i]);  // no other write reaches these slots
+      else my[rslot[i]] = CT(double(my[rslot[i]]) + rsum[i]);
     }
   }
   bpart[u] = bsum;
@@ -823,8 +823,11 @@ __device__ __forceinline__ void bulk_wait_read() {
 }
 
 // One tile: rows [t.n0, t.n1) of test component t.comp.  `acc` holds the
-// tile's CSR value segment followed by one double per row unit (load-vector
-// partials).  blockDim must be at least the tile's unit count.
+// tile's CSR value segment (in the contraction type: the FP32-contraction
+// path also accumulates in FP32 -- about 1e-7 of the row's largest entry,
+// the columns kept in registers summed in FP64) followed by one double per
+// row unit (load-vector partials).  blockDim must be at least the tile's unit
+// count.
 //
 // With Dirichlet data (p.bc_flags) each element row is modified as
 // SystemAssembler::apply_bc (dolfin/fem/SystemAssembler.cpp:1037-1070) does
@@ -834,15 +837,16 @@ __device__ __forceinline__ void bulk_wait_read() {
 template <int D, int P, int FORM, bool KP1, int LOADM, typename CT, int VAR = VAR_BC>
 __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, double* acc) {
   constexpr int BS = FORM == FORM_ELAS ? D : 1;
+  constexpr bool F64 = sizeof(CT) == 8;
   const int32_t r0 = __ldg(p.node_rowptr + t.n0), r1 = __ldg(p.node_rowptr + t.n1);
   const int seg = BS * (r1 - r0);
   double* dst = p.vals + int64_t(t.comp) * p.vstride + int64_t(BS) * r0 - p.vbase;
-  // The segment is staged at the address parity (mod 16 bytes) of its
+  // An FP64 segment is staged at the address parity (mod 16 bytes) of its
   // destination, so that its 16-byte-aligned middle leaves shared memory by
   // one bulk copy (the launch gives one double of slack for the shift).
-  const int sh = int((reinterpret_cast<uintptr_t>(dst) >> 3) & 1u);
-  double* segm = acc + sh;
-  double* bpart = segm + seg;
+  const int sh = F64 ? int((reinterpret_cast<uintptr_t>(dst) >> 3) & 1u) : 0;
+  CT* segm = reinterpret_cast<CT*>(acc) + sh;
+  double* bpart = acc + (sh + seg * int(sizeof(CT)) / 8 + 1);
   const int units = (t.n1 - t.n0) * BS;
   if (int(threadIdx.x) < units) {
     // tiles never mix vertex and edge nodes (the host cuts P2 tiles at the
@@ -854,7 +858,7 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
   }
   // the segment's generic-proxy writes are made visible to the bulk copy
   // (async proxy) by this fence and the barrier
-  bulk_fence();
+  if constexpr (F64) bulk_fence();
   __syncthreads();
   if constexpr (LOADM != LOAD_NONE) {
     // b of each row: its trial blocks' partials in block order
@@ -867,7 +871,9 @@ __device__ __forceinline__ void tile_body(const AsmParams& p, const Tile t, doub
     }
   }
   if (p.add_values) {
-    for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] += segm[i];
+    for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] += double(segm[i]);
+  } else if constexpr (!F64) {
+    for (int i = threadIdx.x; i < seg; i += blockDim.x) dst[i] = double(segm[i]);
   } else {
     // an unaligned first and last double by plain stores, the rest (16-byte
     // aligned at both ends, a multiple of 16 bytes) by one bulk copy that

@@ -89,9 +89,11 @@ void run_assemble(const AsmParams& p, const LaunchCfg& cfg) {
     if (n <= 0) continue;
     AsmParams q = p;
     q.tiles = p.tiles + cb[k];
-    // the class's row segment, one load partial per thread, and 16 bytes of
+    // the class's row segment (class sizes count doubles; the FP32 path
+    // accumulates in floats), one load partial per thread, and 16 bytes of
     // slack for staging the segment at its destination's alignment
-    const size_t smem = size_t((*cfg.class_smem)[k]) + size_t(cfg.threads) * sizeof(double) + 16;
+    const size_t smem = size_t((*cfg.class_smem)[k]) * sizeof(CT) / sizeof(double) +
+                        size_t(cfg.threads) * sizeof(double) + 16;
     cudaStream_t st = cfg.stream;
     if (fork) {
       st = S->s[used];
