@@ -37,13 +37,15 @@ struct BatchTile {
   int32_t n0, n1;
 };
 
+// Members carry no Dirichlet data (their parameters leave bc_flags null), so
+// the tiles run the instantiation without boundary-condition state.
 template <typename CT>
 __device__ __forceinline__ void batch_tile(const BatchMember& m, const Tile& t, double* acc) {
   switch (m.kind) {
-    case KIND_P1TRI: tile_body<2, 1, FORM_DIFF, true, LOAD_NONE, CT>(m.p, t, acc); break;
-    case KIND_P2TRI: tile_body<2, 2, FORM_DIFF, true, LOAD_NONE, CT>(m.p, t, acc); break;
-    case KIND_P1TET: tile_body<3, 1, FORM_DIFF, true, LOAD_NONE, CT>(m.p, t, acc); break;
-    default: tile_body<3, 2, FORM_DIFF, true, LOAD_NONE, CT>(m.p, t, acc); break;
+    case KIND_P1TRI: tile_body<2, 1, FORM_DIFF, true, LOAD_NONE, CT, 0>(m.p, t, acc); break;
+    case KIND_P2TRI: tile_body<2, 2, FORM_DIFF, true, LOAD_NONE, CT, 0>(m.p, t, acc); break;
+    case KIND_P1TET: tile_body<3, 1, FORM_DIFF, true, LOAD_NONE, CT, 0>(m.p, t, acc); break;
+    default: tile_body<3, 2, FORM_DIFF, true, LOAD_NONE, CT, 0>(m.p, t, acc); break;
   }
 }
 
