@@ -53,7 +53,9 @@ __device__ __forceinline__ void batch_tile(const BatchMember& m, const Tile& t, 
 // Register cap 64 (16 resident 64-thread CTAs per SM): the batched members
 // are 2D meshes, whose rows need fewer registers; measured on B200 for 512
 // triangle meshes (ms per graph replay): 0.770 at 64 registers against 0.788
-// at 72, 0.847 at 80 (some spills at 64 and 72, none at 96: 0.975).
+// at 72, 0.847 at 80 (some spills at 64 and 72, none at 96: 0.975); with
+// the tiles' Dirichlet-free instantiation (fewer spills) 0.673 at 64 against
+// 0.716 at 72.
 #ifndef DB2_BATCH_MAXNREG
 #define DB2_BATCH_MAXNREG 64
 #endif
