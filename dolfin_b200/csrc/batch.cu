@@ -196,6 +196,8 @@ int db2_batch_create(int count, const db2_pattern* patterns, const db2_form* for
         if (forms[m].kind != DB2_FORM_DIFFUSION || forms[m].coeff != DB2_COEFF_P1 || P->bs != 1)
           fail(DB2_ERR_UNSUPPORTED, "batch member %d: only kappa*grad.grad with a P1 kappa", m);
         if (!kappas[m] || !vals[m]) fail(DB2_ERR_ARGUMENT, "batch member %d: NULL kappa/vals", m);
+        if (reinterpret_cast<uintptr_t>(vals[m]) % alignof(double))
+          fail(DB2_ERR_ARGUMENT, "batch member %d: vals must be 8-byte aligned", m);
         P->ensure_device();
         if (P->rec_escapes)
           fail(DB2_ERR_UNSUPPORTED,

@@ -139,6 +139,11 @@ void launch_assemble(const Pattern& P, const FormArgs* a, const FormArgs* L, int
                      const double* bc_vals, void* stream) {
   const Space& V = *P.V;
   const int D = V.mesh->tdim;
+  // the tile kernel writes its value segments with 16-byte bulk copies from
+  // an 8-byte-aligned base (and doubles elsewhere): refuse other pointers
+  // here rather than fault on the device
+  if ((reinterpret_cast<uintptr_t>(vals) | reinterpret_cast<uintptr_t>(b)) % alignof(double))
+    fail(DB2_ERR_ARGUMENT, "value and vector arrays must be 8-byte aligned device pointers");
   dev::AsmParams p = make_params(P);
   p.vals = vals;
   p.b = b;

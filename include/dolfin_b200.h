@@ -233,7 +233,9 @@ int db2_pattern_row_block_csr_host(db2_pattern P, int32_t* rowptr, int32_t* cols
 
 /* ---- assembly --------------------------------------------------------- */
 /* Assembler::assemble(A, a) (dolfin/fem/Assembler.cpp:52-103) for a bilinear
-   form on the pattern's space: writes CSR values vals[nnz] (device).  w is
+   form on the pattern's space: writes CSR values vals[nnz] (device, 8-byte
+   aligned like every double array here; other pointers are refused with
+   DB2_ERR_ARGUMENT).  w is
    the device P1 coefficient (kappa) when a.coeff is P1/P1_SCALED.
    add_values as AssemblerBase.h:46 (accumulate into vals). */
 int db2_assemble_matrix(db2_pattern P, const db2_form* a, const double* w, int precision,

@@ -294,3 +294,15 @@ def test_row_range_tiles_cover_exactly_the_range():
     for a, b in [(-1, 3), (5, 4), (0, nn + 1)]:
         with pytest.raises(_capi.DB2Error):
             P.set_row_range(a, b)
+
+
+def test_misaligned_output_arrays_are_refused_on_the_host():
+    """The assembly writes its CSR values with 16-byte bulk copies from an
+    8-byte-aligned base: an output pointer that is not 8-byte aligned is an
+    argument error raised before any device work (no GPU needed here)."""
+    import ctypes as C
+    V = d2.FunctionSpace(d2.UnitSquareMesh(2, 2), "Lagrange", 1)
+    a = _capi.make_form(_capi.FORM_DIFFUSION, _capi.COEFF_NONE, (1.0,))
+    with pytest.raises(_capi.DB2Error, match="8-byte aligned"):
+        _capi.call("db2_assemble_matrix", V.pattern().handle, C.byref(a), None, _capi.FP64,
+                   C.c_void_p(0x1004), 0, None)
