@@ -104,3 +104,33 @@ def test_row_blocks_held_alone_equal_full(kind, nranks):
             d2.SystemAssembler(a, L, bcs).assemble(A, b)
         finally:
             P.set_row_range(0, nn)
+
+
+@pytest.mark.parametrize("kind", ["p2", "elas", "p2bc"])
+def test_fp32_row_blocks_equal_fp32_full(kind):
+    """The FP32-contraction path (FP32 row segments, converted on the way
+    out) through row-block storage: the blocks placed back at their global
+    rows equal the FP32 whole-matrix assembly bit for bit."""
+    V, a, L, bcs = _problem(kind)
+    A, b = d2.SystemAssembler(a, L, bcs, "fp32").assemble()
+    ref_vals, ref_b = A.values_tensor().cpu().numpy(), b.get_local()
+    P = A.pattern
+    frp, _ = P.csr_host()
+    nn = V.dim() // V.value_size()
+    cuts = shard.row_partition(P.plan()["inc_ptr"], 3)
+    vals = np.full(len(ref_vals), np.nan)
+    bv = np.full(len(ref_b), np.nan)
+    try:
+        for r in range(3):
+            blk = shard.RowBlock(V, int(cuts[r]), int(cuts[r + 1]))
+            bvals, bb = blk.assemble_system(a, L, bcs, precision="fp32")
+            torch.cuda.synchronize()
+            rp, _ = blk.csr_host()
+            bvals, bb = bvals.cpu().numpy(), bb.cpu().numpy()
+            for i, dof in enumerate(blk.dofs()):
+                vals[frp[dof]:frp[dof + 1]] = bvals[rp[i]:rp[i + 1]]
+            bv[blk.dofs()] = bb
+    finally:
+        P.set_row_range(0, nn)
+    assert np.array_equal(vals, ref_vals)
+    assert np.array_equal(bv, ref_b)
