@@ -3,6 +3,8 @@
 // coefficient.
 #include <cuda_runtime.h>
 
+#include <utility>
+
 #include "launch.cuh"
 #include "action_tc.cuh"
 
@@ -253,78 +255,117 @@ __global__ void __launch_bounds__(256) k_apply_gather(const uint32_t* __restrict
   for (int c = 0; c < BS; ++c) y[int64_t(c) * nnodes + node] = acc[c];
 }
 
+// Adjoint, step 1, the part of local node LI of the cell (a compile-time
+// relabelling, so the permuted geometry tensor is register renaming):
+// acc[a] += sum_j gA_(LI,j) dA^K_(LI,j)/dkappa_a + gb_LI db^K_LI/dkappa_a.
+// Wn[a][b] = n_a . n_b in the cell's own vertex order; under the relabelling
+// n'_a = +-n_perm[a], so W'_ab = Wn[perm[a]][perm[b]] (|det J| unchanged).
+template <int D, int P, bool LOADK, typename CT, int LI>
+__device__ __forceinline__ void vjp_node(const AsmParams& p, int64_t cell,
+                                         const double (&Wn)[D + 1][D + 1], double s, double vol,
+                                         const double (&fv)[D + 1], const double* __restrict__ gA,
+                                         const double* __restrict__ gb, double (&acc)[D + 1]) {
+  using E = El<D, P>;
+  using R = Rows<D, P, CT>;
+  constexpr int NB = D + 1;
+  constexpr uint32_t code = perm_code(D, LI);
+  constexpr bool vertex = LI <= D;
+  const uint32_t ii = __ldg(p.cell_inc + size_t(cell) * E::K + LI);
+  const uint32_t node = __ldg(p.cell_nodes + size_t(cell) * E::K + LI);
+  const double* grow = gA + __ldg(p.node_rowptr + node);
+  // gA at the row's slots, in the relabelled local order
+  double g[E::K];
+  const Rec<D, P> rr = load_rec<D, P>(p, rec_index<D, P>(p, node, ii - __ldg(p.inc_ptr + node)));
+#pragma unroll
+  for (int j = 0; j < E::K; ++j) g[j] = __ldg(grow + rr.slot(j));
+  auto pm = [](int a) { return int((code >> (2 * a)) & 3u); };
+  CT W0[1][NB];
+  CT W1[2][NB];
+  // W times the generated rows' scale (see element_rows.h)
+  const double sv = s * (p.kscale * R::sv_kp1);
+#pragma unroll
+  for (int b = 0; b < NB; ++b) W0[0][b] = CT(Wn[pm(0)][pm(b)] * sv);
+  if constexpr (P == 2) {
+    const double se = s * (p.kscale * R::se_kp1);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < NB; ++b) W1[a][b] = CT(Wn[pm(a)][pm(b)] * se);
+  }
+  CT lk[NB];
+  if constexpr (LOADK) {
+    CT fc[NB];
+#pragma unroll
+    for (int a = 0; a < NB; ++a) fc[a] = CT(fv[pm(a)]);
+    if constexpr (P == 2 && !vertex) R::e_kfp1(fc, lk);
+    else R::v_kfp1(fc, lk);
+  }
+  const double gbi = LOADK ? __ldg(gb + node) : 0.0;
+#pragma unroll
+  for (int m = 0; m < NB; ++m) {
+    CT unit[NB];
+#pragma unroll
+    for (int a = 0; a < NB; ++a) unit[a] = CT(a == m ? 1 : 0);
+    CT d[E::K];
+    if constexpr (P == 1 || vertex) R::v_kp1(W0, unit, d);
+    else R::e_kp1(W1, unit, d);
+    double t = 0.0;
+#pragma unroll
+    for (int j = 0; j < E::K; ++j) t = fma(g[j], double(d[j]), t);
+    if constexpr (LOADK) t = fma(gbi, vol * double(lk[m]) * p.fc[0], t);
+    // relabelled vertex m is original local vertex perm[m]
+    acc[pm(m)] += t;
+  }
+}
+
+template <int D, int P, bool LOADK, typename CT, int... LI>
+__device__ __forceinline__ void vjp_nodes(const AsmParams& p, int64_t cell,
+                                          const double (&Wn)[D + 1][D + 1], double s, double vol,
+                                          const double (&fv)[D + 1], const double* gA,
+                                          const double* gb, double (&acc)[D + 1],
+                                          std::integer_sequence<int, LI...>) {
+  (vjp_node<D, P, LOADK, CT, LI>(p, cell, Wn, s, vol, fv, gA, gb, acc), ...);
+}
+
 // Adjoint, step 1 (one thread per cell): t[cell][m] = sum_{i,j in cell}
 // gA_ij dA^K_ij/dkappa_m + sum_i gb_i db^K_i/dkappa_m for the P1 kappa
-// basis functions m of the cell.
+// basis functions m of the cell.  The cell's vertices and geometry are
+// loaded and computed once; each local node's relabelled geometry tensor is
+// a permutation of the cell's.
+// Register caps: the P2 node parts (ten of them, inlined) would take up to
+// 174 registers uncapped; P1 cells need no more than 64.
+template <int P>
+constexpr int vjp_maxnreg() {
+  return P == 1 ? 64 : 128;
+}
 template <int D, int P, bool LOADK, typename CT>
-__global__ void __launch_bounds__(256) k_vjp_cells(const AsmParams p, int64_t ncells,
+__global__ void __maxnreg__((vjp_maxnreg<P>())) k_vjp_cells(const AsmParams p, int64_t ncells,
                                                    const double* __restrict__ gA,
                                                    const double* __restrict__ gb,
                                                    double* __restrict__ t) {
   using E = El<D, P>;
-  using R = Rows<D, P, CT>;
   constexpr int NB = D + 1;
   const int64_t cell = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (cell >= ncells) return;
-  double acc[NB];
-  for (int a = 0; a < NB; ++a) acc[a] = 0.0;
-  const uint32_t* cn = p.cell_nodes + size_t(cell) * E::K;
-  for (int li = 0; li < E::K; ++li) {
-    const uint32_t ii = __ldg(p.cell_inc + size_t(cell) * E::K + li);
-    const uint32_t node = __ldg(cn + li);
-    const double* grow = gA + __ldg(p.node_rowptr + node);
-    const uint32_t code = perm_of<D>(li);
-    uint32_t v[D + 1], pv[D + 1];
-    load_verts<D>(p, uint32_t(cell), v);
-    relabel<D>(v, code, pv);
-    double x[D + 1][D], kap_unused[D + 1], f_unused[D + 1];
-    load_vertex_data<D, false>(p, pv, x, kap_unused, f_unused);
-    Geometry<D> G;
-    geometry(x, G);
-    const bool vertex = li <= D;
-    // gA at the row's slots, in the relabelled local order
-    double g[E::K];
-    const Rec<D, P> rr = load_rec<D, P>(p, rec_index<D, P>(p, node, ii - __ldg(p.inc_ptr + node)));
+  uint32_t v[NB];
+  load_verts<D>(p, uint32_t(cell), v);
+  double x[NB][D], kap_unused[NB], f_unused[NB];
+  load_vertex_data<D, false>(p, v, x, kap_unused, f_unused);
+  double fv[NB];
 #pragma unroll
-    for (int j = 0; j < E::K; ++j) g[j] = __ldg(grow + rr.slot(j));
-    CT W0[1][NB];
-    CT W1[2][NB];
-    // W times the generated rows' scale (see element_rows.h)
-    for (int b = 0; b < NB; ++b) W0[0][b] = CT(ndot<D>(G, 0, b) * (G.s * (p.kscale * R::sv_kp1)));
-    if constexpr (P == 2)
-      for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < NB; ++b)
-          W1[a][b] = CT(ndot<D>(G, a, b) * (G.s * (p.kscale * R::se_kp1)));
-    double fv[NB];
-    if constexpr (LOADK)
-      for (int a = 0; a < NB; ++a) fv[a] = __ldg(p.f + pv[a]);
-    CT lk[NB];
-    if constexpr (LOADK) {
-      CT fc[NB];
-      for (int a = 0; a < NB; ++a) fc[a] = CT(fv[a]);
-      if constexpr (P == 2) {
-        if (vertex) R::v_kfp1(fc, lk);
-        else R::e_kfp1(fc, lk);
-      } else {
-        R::v_kfp1(fc, lk);
-      }
-    }
-    const double gbi = LOADK ? __ldg(gb + node) : 0.0;
-    for (int m = 0; m < NB; ++m) {
-      CT unit[NB];
-      for (int a = 0; a < NB; ++a) unit[a] = CT(a == m ? 1 : 0);
-      CT d[E::K];
-      if (P == 1 || vertex) R::v_kp1(W0, unit, d);
-      else if constexpr (P == 2) R::e_kp1(W1, unit, d);
-      double s = 0.0;
-      for (int j = 0; j < E::K; ++j) s = fma(g[j], double(d[j]), s);
-      if constexpr (LOADK) s = fma(gbi, G.vol * double(lk[m]) * p.fc[0], s);
-      // relabelled vertex m is original local vertex perm[m]
-      const int orig = int((code >> (2 * m)) & 3u);
-      for (int a = 0; a < NB; ++a)
-        if (a == orig) acc[a] += s;
-    }
-  }
+  for (int a = 0; a < NB; ++a) fv[a] = LOADK ? __ldg(p.f + v[a]) : 0.0;
+  Geometry<D> G;
+  geometry(x, G);
+  double Wn[NB][NB];
+#pragma unroll
+  for (int a = 0; a < NB; ++a)
+#pragma unroll
+    for (int b = a; b < NB; ++b) Wn[a][b] = Wn[b][a] = ndot<D>(G, a, b);
+  double acc[NB];
+#pragma unroll
+  for (int a = 0; a < NB; ++a) acc[a] = 0.0;
+  vjp_nodes<D, P, LOADK, CT>(p, cell, Wn, G.s, G.vol, fv, gA, gb, acc,
+                             std::make_integer_sequence<int, E::K>{});
   // in vertex-incidence order (vertex nodes come first in the node-contiguous
   // incidence array), so that step 2 reads each vertex's terms contiguously
   for (int a = 0; a < NB; ++a) t[__ldg(p.cell_inc + size_t(cell) * E::K + a)] = acc[a];
