@@ -122,8 +122,24 @@ __device__ __forceinline__ void test_basis(const CT (&S)[D + 1], const double (&
   }
 }
 
+// Block size and register cap of step 1.  Residency is set per SM
+// sub-partition (16,384 registers: 5 warps at 81-96 registers per thread,
+// 6 at up to 80) and in whole blocks.
+#ifndef DB2_APPLY_THREADS
+#define DB2_APPLY_THREADS 128
+#endif
+#ifndef DB2_APPLY_MAXNREG_P2DIFF
+#define DB2_APPLY_MAXNREG_P2DIFF 80
+#endif
+#ifndef DB2_APPLY_MAXNREG_ELAS
+#define DB2_APPLY_MAXNREG_ELAS 128
+#endif
+template <int P, int FORM>
+constexpr int apply_maxnreg() {
+  return FORM == FORM_ELAS ? DB2_APPLY_MAXNREG_ELAS : P == 2 ? DB2_APPLY_MAXNREG_P2DIFF : 255;
+}
 template <int D, int P, int FORM, bool KP1, typename CT>
-__global__ void __launch_bounds__(256) k_apply_cells(const AsmParams p, int64_t ncells,
+__global__ void __maxnreg__((apply_maxnreg<P, FORM>())) k_apply_cells(const AsmParams p, int64_t ncells,
                                                      const double* __restrict__ xin,
                                                      double* __restrict__ ycell) {
   constexpr int NB = D + 1, K = El<D, P>::K;
@@ -394,7 +410,8 @@ void run_apply(const Pattern& Pt, const AsmParams& p, const double* x, double* y
   double* ycell = Pt.d_cellvals.as<double>();
   const int64_t threads = nc * (FORM == FORM_ELAS ? D : 1);
   if (threads > 0) {
-    k_apply_cells<D, P, FORM, KP1, CT><<<unsigned((threads + 255) / 256), 256, 0, s>>>(p, nc, x, ycell);
+    constexpr int bt = DB2_APPLY_THREADS;
+    k_apply_cells<D, P, FORM, KP1, CT><<<unsigned((threads + bt - 1) / bt), bt, 0, s>>>(p, nc, x, ycell);
     count_launch();
     check_cuda("apply launch");
   }
