@@ -593,18 +593,23 @@ def extra_config5(args, flush, peak, rank):
            "algorithmic_bytes": by, "setup_s": round(w["setup_s"], 2)}
     out["traffic"], out["traffic_source"] = profiled_traffic("poisson_p2_96")
     out["matrix_free"] = measure_action(w, args, flush, peak, repeats=100)
-    # the FP32-contraction action: reference tensor x geometry tensor on the
-    # tensor cores (tcgen05), against the FP64 action
-    tc = measure_action(w, args, flush, peak, repeats=100, precision="fp32")
     import dolfin_b200 as d2
     x = torch.randn(w["V"].dim(), dtype=torch.float64, device="cuda",
                     generator=torch.Generator("cuda").manual_seed(7))
     y64 = d2.assemble_action(w["a"], d2.Vector(x)).tensor().clone()
-    y32 = d2.assemble_action(w["a"], d2.Vector(x), precision="fp32").tensor()
-    tc["max_rel_err_vs_fp64"] = float((y32 - y64).abs().max() / y64.abs().max())
-    tc["speedup_vs_fp64"] = round(out["matrix_free"]["ms_per_action"] / tc["ms_per_action"], 3)
-    tc["contraction"] = "tcgen05 kind::f16, two half limbs of the FP64 geometry tensor, FP32 accumulation"
-    out["matrix_free_fp32_tensor_core"] = tc
+    # the FP32-contraction actions against the FP64 one: element actions by
+    # FP32 quadrature ("fp32", the default FP32 path), and the reference
+    # tensor x geometry tensor on the tensor cores (tcgen05, "fp32_tc")
+    for key, prec, how in (
+            ("matrix_free_fp32", "fp32", "FP32 quadrature from the FP64 geometry, FP32 element actions"),
+            ("matrix_free_fp32_tensor_core", "fp32_tc",
+             "tcgen05 kind::f16, two half limbs of the FP64 geometry tensor, FP32 accumulation")):
+        r = measure_action(w, args, flush, peak, repeats=100, precision=prec)
+        y32 = d2.assemble_action(w["a"], d2.Vector(x), precision=prec).tensor()
+        r["max_rel_err_vs_fp64"] = float((y32 - y64).abs().max() / y64.abs().max())
+        r["speedup_vs_fp64"] = round(out["matrix_free"]["ms_per_action"] / r["ms_per_action"], 3)
+        r["contraction"] = how
+        out[key] = r
     del w
     torch.cuda.empty_cache()
     return out
@@ -730,11 +735,11 @@ def run_profile(args):
     import torch
     import dolfin_b200 as d2
     w = setup_workload(args.workload, seed=1, device=None, n_override=args.mesh_n)
-    if args.profile in ("action", "action32"):
+    if args.profile in ("action", "action32", "action32q"):
         x = torch.randn(w["V"].dim(), dtype=torch.float64, device="cuda",
                         generator=torch.Generator("cuda").manual_seed(3))
         xv, y = d2.Vector(x), d2.Vector(n=w["V"].dim())
-        prec = "fp32" if args.profile == "action32" else "fp64"
+        prec = {"action": "fp64", "action32": "fp32_tc", "action32q": "fp32"}[args.profile]
         fn = lambda: d2.assemble_action(w["a"], xv, y, precision=prec)
     else:
         fn = lambda: w["S"].assemble(w["A"], w["b"])
@@ -755,7 +760,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the P2 n=96 and adjoint measurements of the default line")
-    ap.add_argument("--profile", choices=["step", "action", "action32"], default=None,
+    ap.add_argument("--profile", choices=["step", "action", "action32", "action32q"], default=None,
                     help="run only the hot loop (for ncu), print no JSON")
     ap.add_argument("--mesh-n", type=int, default=None, help="mesh size override (with --profile)")
     ap.add_argument("--split", choices=["replicas", "rows"], default="replicas",
@@ -841,8 +846,18 @@ def main():
     err32 = float((A32.values_tensor() - vals64).abs().max().item() / vals64.abs().max().item())
     del A32, vals64
 
-    # matrix-free action on the same form
+    # matrix-free action on the same form, FP64 and with the FP32 element
+    # actions (FP32 quadrature from the FP64 geometry)
     mf = measure_action(w, args, flush, peak)
+    mf32 = measure_action(w, args, flush, peak, precision="fp32")
+    xa = torch.randn(w["V"].dim(), dtype=torch.float64, device="cuda",
+                     generator=torch.Generator("cuda").manual_seed(7))
+    ya64 = d2.assemble_action(w["a"], d2.Vector(xa)).tensor().clone()
+    ya32 = d2.assemble_action(w["a"], d2.Vector(xa), precision="fp32").tensor()
+    mf["fp32"] = {"ms_per_action": mf32["ms_per_action"], "mcells_s": mf32["mcells_s"],
+                  "speedup_vs_fp64": round(mf["ms_per_action"] / mf32["ms_per_action"], 3),
+                  "max_rel_err_vs_fp64": float((ya32 - ya64).abs().max() / ya64.abs().max())}
+    del xa, ya64, ya32
 
     # end to end through the public API with host buffers: per step, H2D of the
     # step's input (vertex coordinates for elasticity, kappa and f otherwise)

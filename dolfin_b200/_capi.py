@@ -19,7 +19,7 @@ ERR_NAMES = {1: "argument", 2: "shape", 3: "index", 4: "mesh", 5: "unsupported",
 FORM_DIFFUSION, FORM_LOAD, FORM_ELASTICITY = 1, 2, 3
 FORM_FACET_MASS, FORM_FACET_LOAD, FORM_FUNCTIONAL, FORM_FACET_FUNCTIONAL = 4, 5, 6, 7
 COEFF_NONE, COEFF_CONSTANT, COEFF_P1, COEFF_P1_SCALED, COEFF_COORD, COEFF_P1_KAPPA = 0, 1, 2, 3, 4, 5
-FP64, FP32_CONTRACT = 0, 1
+FP64, FP32_CONTRACT, FP32_TENSOR_CORE = 0, 1, 2
 
 
 class DB2Form(C.Structure):

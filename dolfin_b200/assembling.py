@@ -18,7 +18,10 @@ from ._capi import call
 from .la import Matrix, Vector
 from .ufl import Form, Recognised, recognise_functional, recognise_parts
 
-_PREC = {"fp64": _capi.FP64, "fp32": _capi.FP32_CONTRACT, None: _capi.FP64}
+# "fp32_tc" (the matrix-free action of P2 diffusion only): the FP32
+# contraction on the tensor cores
+_PREC = {"fp64": _capi.FP64, "fp32": _capi.FP32_CONTRACT, "fp32_tc": _capi.FP32_TENSOR_CORE,
+         None: _capi.FP64}
 
 
 def _stream():

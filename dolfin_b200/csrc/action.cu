@@ -141,7 +141,7 @@ constexpr int apply_maxnreg() {
 template <int D, int P, int FORM, bool KP1, typename CT>
 __global__ void __maxnreg__((apply_maxnreg<P, FORM>())) k_apply_cells(const AsmParams p, int64_t ncells,
                                                      const double* __restrict__ xin,
-                                                     double* __restrict__ ycell) {
+                                                     CT* __restrict__ ycell) {
   constexpr int NB = D + 1, K = El<D, P>::K;
   constexpr bool ELAS = FORM == FORM_ELAS;
   constexpr int BS = ELAS ? D : 1;
@@ -405,9 +405,11 @@ template <int D, int P, int FORM, bool KP1, typename CT>
 void run_apply(const Pattern& Pt, const AsmParams& p, const double* x, double* y, cudaStream_t s) {
   constexpr int K = El<D, P>::K, BS = FORM == FORM_ELAS ? D : 1, n = BS * K;
   const int64_t nc = Pt.V->mesh->nc;
-  const size_t need = size_t(nc) * n * sizeof(double);
+  // element actions in the contraction type (the FP32 path moves half the
+  // bytes); the ordered gather sums them in FP64
+  const size_t need = size_t(nc) * n * sizeof(CT);
   if (Pt.d_cellvals.bytes < need) Pt.d_cellvals.alloc(need);
-  double* ycell = Pt.d_cellvals.as<double>();
+  CT* ycell = Pt.d_cellvals.as<CT>();
   const int64_t threads = nc * (FORM == FORM_ELAS ? D : 1);
   if (threads > 0) {
     constexpr int bt = DB2_APPLY_THREADS;
@@ -415,7 +417,7 @@ void run_apply(const Pattern& Pt, const AsmParams& p, const double* x, double* y
     count_launch();
     check_cuda("apply launch");
   }
-  k_apply_gather<BS, K, FORM != FORM_ELAS><<<unsigned((p.nnodes + 255) / 256), 256, 0, s>>>(
+  k_apply_gather<BS, K, FORM != FORM_ELAS, CT><<<unsigned((p.nnodes + 255) / 256), 256, 0, s>>>(
       p.inc_ptr, p.inc, p.nnodes, ycell, y);
   count_launch();
   check_cuda("apply gather launch");
@@ -465,7 +467,8 @@ void launch_apply(const Pattern& P, const FormArgs& a, int precision, const doub
   dev::AsmParams p = make_params(P);
   const int D = P.V->mesh->tdim, deg = P.V->degree;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const bool fp32 = precision == DB2_FP32_CONTRACT;
+  const bool tc = precision == DB2_FP32_TENSOR_CORE;
+  const bool fp32 = precision == DB2_FP32_CONTRACT || tc;
   if (precision != DB2_FP64 && !fp32) fail(DB2_ERR_ARGUMENT, "unknown precision %d", precision);
   bool kp1 = false;
   if (a.f.kind == DB2_FORM_DIFFUSION) {
@@ -475,7 +478,9 @@ void launch_apply(const Pattern& P, const FormArgs& a, int precision, const doub
     if (kp1 && !a.w) fail(DB2_ERR_ARGUMENT, "P1 coefficient field missing");
     p.kappa = a.w;
     pack_vertex_records(P, kp1 ? a.w : nullptr, nullptr, stream);
-    if (fp32 && D == 3 && deg == 2) {
+    if (tc) {
+      if (D != 3 || deg != 2)
+        fail(DB2_ERR_UNSUPPORTED, "the tensor-core action is for P2 tetrahedra");
       // FP32 contraction on the tensor cores
       if (kp1) dev::run_apply_tc<true>(P, p, x, y, s);
       else dev::run_apply_tc<false>(P, p, x, y, s);
@@ -496,6 +501,7 @@ void launch_apply(const Pattern& P, const FormArgs& a, int precision, const doub
 #undef DB2_AP
   } else if (a.f.kind == DB2_FORM_ELASTICITY) {
     if (D != 3 || P.bs != 3) fail(DB2_ERR_UNSUPPORTED, "elasticity needs a 3D vector space");
+    if (tc) fail(DB2_ERR_UNSUPPORTED, "the tensor-core action is for P2 diffusion");
     p.mu = a.f.mu;
     p.lmbda = a.f.lmbda;
     if (deg == 1) {
@@ -539,7 +545,8 @@ void launch_vjp(const Pattern& P, const FormArgs& a, const FormArgs& L, int prec
     fail(DB2_ERR_UNSUPPORTED, "the adjoint is provided for kappa*grad(u).grad(v)*dx on scalar spaces");
   if (!(a.f.coeff == DB2_COEFF_P1 || a.f.coeff == DB2_COEFF_P1_SCALED))
     fail(DB2_ERR_ARGUMENT, "the adjoint is with respect to a P1 kappa");
-  const bool fp32 = precision == DB2_FP32_CONTRACT;
+  const bool tc = precision == DB2_FP32_TENSOR_CORE;
+  const bool fp32 = precision == DB2_FP32_CONTRACT || tc;
   if (precision != DB2_FP64 && !fp32) fail(DB2_ERR_ARGUMENT, "unknown precision %d", precision);
   dev::AsmParams p = make_params(P);
   p.kscale = a.f.coeff == DB2_COEFF_P1_SCALED ? a.f.constant[0] : 1.0;

@@ -74,8 +74,10 @@ enum db2_coeff_kind {
 };
 enum db2_precision {
   DB2_FP64 = 0,            /* geometry, contraction, accumulation in FP64    */
-  DB2_FP32_CONTRACT = 1    /* FP64 geometry and global accumulation; the
+  DB2_FP32_CONTRACT = 1,   /* FP64 geometry and global accumulation; the
                               reference-tensor contraction in FP32           */
+  DB2_FP32_TENSOR_CORE = 2 /* db2_apply only, P2 tetrahedra, kappa*grad.grad:
+                              the FP32 contraction on the tensor cores      */
 };
 
 typedef struct {
@@ -295,13 +297,16 @@ int db2_assemble_facets_bc(db2_pattern P, const db2_form* a_ds, const double* wa
    pattern; calls on one pattern that overlap on the GPU race on it. */
 int db2_apply(db2_pattern P, const db2_form* a, const double* w, int precision, const double* x,
               double* y, void* stream);
-/* db2_apply with DB2_FP32_CONTRACT on P2 tetrahedra (kappa*grad.grad, kappa
-   1, Constant or P1) contracts the reference tensor with the geometry tensor
-   on the tensor cores (tcgen05, half-precision limb pairs of the FP64
-   geometry, FP32 accumulation: about 3e-7 of the entries' scale).  Its
-   waits on the tensor core are bounded; *status = 1 reports that one ran
-   out (the outputs of that call are NaN), 0 that none has.  Synchronises the
-   device.  No counterpart in the reference. */
+/* db2_apply with DB2_FP32_CONTRACT computes the element actions in FP32
+   from the FP64 geometry and keeps them in FP32 until the FP64 row sums.
+   With DB2_FP32_TENSOR_CORE (P2 tetrahedra, kappa*grad.grad, kappa 1,
+   Constant or P1; other forms are refused) it contracts the reference
+   tensor with the geometry tensor on the tensor cores instead (tcgen05,
+   half-precision limb pairs of the FP64 geometry, FP32 accumulation: about
+   3e-7 of the entries' scale).  Its waits on the tensor core are bounded;
+   *status = 1 reports that one ran out (the outputs of that call are NaN),
+   0 that none has.  Synchronises the device.  No counterpart in the
+   reference. */
 int db2_tensor_core_status(int* status);
 /* Vector-Jacobian product of (A(kappa), b(kappa)) for a = kappa grad.grad
    (P1 kappa) and L = f v dx, or the kappa-weighted load

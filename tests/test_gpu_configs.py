@@ -177,6 +177,8 @@ def test_config5_p2_poisson_full(orc):
     assert _action_err(rp, cols, ovals, xv, y) <= 1e-12
     y32 = d2.assemble_action(a, d2.Vector(torch.as_tensor(xv, device="cuda")), precision="fp32").get_local()
     assert _action_err(rp, cols, ovals, xv, y32) <= FP32_TOL
+    ytc = d2.assemble_action(a, d2.Vector(torch.as_tensor(xv, device="cuda")), precision="fp32_tc").get_local()
+    assert _action_err(rp, cols, ovals, xv, ytc) <= FP32_TOL
 
 
 @pytest.mark.parametrize("precision,tol_oracle,tol_fd", [("fp64", 1e-12, 1e-8), ("fp32", 1e-6, 1e-6)])

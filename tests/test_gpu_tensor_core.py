@@ -1,4 +1,5 @@
-"""The tensor-core (tcgen05) FP32-contraction matrix-free action of
+"""The tensor-core (tcgen05) FP32-contraction matrix-free action (precision
+"fp32_tc") of
 kappa*grad(u).grad(v)*dx on P2 tetrahedra against the oracle's CSR times x:
 |y - R x| <= 1e-6 sum_j |R_ij x_j| per row, with a P1 kappa and with a
 constant one, on meshes whose cell count is and is not a multiple of the
@@ -47,14 +48,18 @@ def test_tensor_core_action_matches_oracle(orc, n, kappa_kind):
     R = sp.csr_matrix((ref, cols, rp), shape=(N, N))
     xv = np.random.default_rng(42).standard_normal(N)
     xt = d2.Vector(torch.as_tensor(xv, device="cuda"))
-    y = d2.assemble_action(a, xt, precision="fp32").get_local()
-    y2 = d2.assemble_action(a, xt, precision="fp32").get_local()
+    y = d2.assemble_action(a, xt, precision="fp32_tc").get_local()
+    y2 = d2.assemble_action(a, xt, precision="fp32_tc").get_local()
     assert _status() == 0
     assert np.array_equal(y, y2)
     mag = abs(R) @ np.abs(xv)
     err = float(np.max(np.abs(y - R @ xv) / mag))
     assert err <= 1e-6, err
-    # and it is the FP32 path, not the FP64 one: they differ
+    # and it is the tensor-core path, neither the FP64 one nor the FP32
+    # quadrature one: they differ
     y64 = d2.assemble_action(a, xt).get_local()
     assert float(np.max(np.abs(y64 - R @ xv) / mag)) <= 1e-12
     assert not np.array_equal(y, y64)
+    y32 = d2.assemble_action(a, xt, precision="fp32").get_local()
+    assert float(np.max(np.abs(y32 - R @ xv) / mag)) <= 1e-6
+    assert not np.array_equal(y, y32) and not np.array_equal(y32, y64)
