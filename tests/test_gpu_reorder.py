@@ -125,3 +125,27 @@ def test_reordered_action_adjoint_and_facets(orc, reordered):
     M = d2.assemble(2.0 * u * v * d2.ds)
     refm = orc.assemble_matrix(orc.form(orc.FACET_MASS, 3, 2, coeff=orc.COEFF_CONST, c=(2.0,)), om, od, od, rp, cols)
     assert _row_err(rp, M.data()[2], refm) <= TOL
+
+
+def test_reordered_fp32_paths(orc, reordered):
+    """The FP32-contraction assembly and both FP32 matrix-free actions (FP32
+    quadrature, tensor cores) on a reordered space, against the FP64 results
+    there: 1e-6 of the row scale (|A| |x| for the actions)."""
+    mesh, om = _case(orc, 3, 4)
+    V = d2.FunctionSpace(mesh, "Lagrange", 2)
+    W = d2.FunctionSpace(mesh, "Lagrange", 1)
+    u, v = d2.TrialFunction(V), d2.TestFunction(V)
+    kappa = _p1_function(W, synthetic.lognormal_field(om.nv, 0.5, 37))
+    a = kappa * d2.inner(d2.grad(u), d2.grad(v)) * d2.dx
+    A = d2.assemble(a)
+    rp, cols, vals = A.data()
+    A32 = d2.assemble(a, precision="fp32")
+    assert _row_err(rp, A32.data()[2], vals) <= 1e-6
+    x = torch.randn(V.dim(), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(38))
+    S = A.sparray()
+    xn = x.cpu().numpy()
+    yref = S @ xn
+    mag = abs(S) @ np.abs(xn)
+    for prec in ("fp32", "fp32_tc"):
+        y = d2.assemble_action(a, d2.Vector(x), precision=prec).get_local()
+        assert float(np.max(np.abs(y - yref) / mag)) <= 1e-6, prec
